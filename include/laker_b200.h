@@ -1,0 +1,216 @@
+/*
+ * laker_b200.h - C ABI of liblaker_b200.so, the B200 (sm_100a) implementation
+ * of the LAKER exact-kernel solve path:
+ *
+ *   - the matrix-free attention-kernel operator  A = lambda*I + exp(E E^T)
+ *     applied to PositionEmbedding outputs E (n x d, d <= 16),
+ *   - the preconditioned conjugate gradient loop (single and batched RHS),
+ *   - application of the factored CCCP preconditioner
+ *     P = c^-1/2 I + Q V diag(lambda_i^-1/2 - c^-1/2) V^T Q^T.
+ *
+ * Conventions
+ *   - Every pointer argument is DEVICE memory unless stated otherwise.  The
+ *     caller owns (allocates and frees) every buffer, including workspaces;
+ *     the library never calls cudaMalloc/cudaFree.  Workspace sizes come from
+ *     the matching *_workspace_bytes query.
+ *   - Matrices are row-major with an explicit leading dimension (elements).
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream).  Calls are
+ *     asynchronous on that stream except laker_pcg_solve, which synchronises
+ *     the stream to poll convergence and returns when the solve has ended.
+ *   - Every entry point returns a laker status code (0 = LAKER_OK).  Kernels
+ *     never trap; device-side failures (a bounded wait that expired) are
+ *     reported through the status code after the stream synchronises.
+ *
+ * Reference interfaces cited as path:line are in the LAKER Python package
+ * (laker/kernels.py, laker/solvers.py, laker/preconditioner.py, laker/core.py).
+ */
+#ifndef LAKER_B200_H
+#define LAKER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                              */
+/* ------------------------------------------------------------------------ */
+enum laker_status {
+  LAKER_OK = 0,
+  LAKER_ERR_INVALID_ARG = 1,   /* bad size, NULL pointer, misaligned buffer  */
+  LAKER_ERR_CUDA = 2,          /* a CUDA runtime call failed                 */
+  LAKER_ERR_BREAKDOWN = 3,     /* PCG: p^T A p <= -eps ||p|| ||Ap||          */
+  LAKER_ERR_NOT_CONVERGED = 4, /* PCG: max_iter reached (x is still valid)   */
+  LAKER_ERR_NONFINITE = 5,     /* PCG: NaN/Inf in an inner product           */
+  LAKER_ERR_TIMEOUT = 6,       /* a bounded device wait expired              */
+  LAKER_ERR_WORKSPACE = 7,     /* workspace smaller than the query returned  */
+  LAKER_ERR_UNSUPPORTED = 8    /* shape/dtype combination not implemented    */
+};
+
+/* Library version as 10000*major + 100*minor + patch. */
+int laker_version(void);
+
+/* Human-readable name of a status code (static storage). */
+const char* laker_status_string(int status);
+
+/* cudaError_t of the most recent LAKER_ERR_CUDA on the calling thread. */
+int laker_last_cuda_error(void);
+
+/* ------------------------------------------------------------------------ */
+/* Embedding layouts                                                         */
+/* ------------------------------------------------------------------------ */
+/* The kernels read embeddings in two packed layouts produced on the device:
+ *   packed32: FP32, point pairs interleaved per dimension
+ *             block q = {e[2q][0], e[2q+1][0], e[2q][1], e[2q+1][1], ...},
+ *             dimension padded to an even count, pair count padded to whole
+ *             256-column tiles with zero points;
+ *   packed64: FP64, one row per point (dimension padded to even), row count
+ *             padded to whole 128-row tiles with zero points.
+ * `E` is an (n x d) row-major matrix with leading dimension ld >= d, either
+ * float (e_is_f64 = 0) or double (e_is_f64 = 1).  1 <= d <= 16.
+ */
+size_t laker_packed32_floats(int64_t n, int d);
+size_t laker_packed64_doubles(int64_t n, int d);
+int laker_pack_f32(const void* E, int e_is_f64, int64_t n, int d, int64_t ld, float* packed32,
+                   void* stream);
+int laker_pack_f64(const void* E, int e_is_f64, int64_t n, int d, int64_t ld, double* packed64,
+                   void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Attention-kernel operator                                                 */
+/* ------------------------------------------------------------------------ */
+/* Workspace for laker_attn_matvec_f32 / _f64 (partial row sums of the column
+ * segments).  precision is 32 or 64. */
+size_t laker_matvec_workspace_bytes(int64_t m, int64_t n, int d, int k, int precision);
+
+/* FP32 fused matvec ("sloppy" operator used inside the PCG loop).
+ *   Y = lam * X[:m] + exp(Er Ec^T) X          (X: n x k, Y: m x k)
+ * Er/Ec are packed32 buffers of m and n points.  lam is applied only when
+ * m == n (pass 0 for a rectangular product such as prediction).  clamp = 1
+ * clamps the Gram entry at 80 before exp, as the reference does when
+ * max ||e||^2 >= 80.  The n x n kernel matrix is never stored.
+ * Replaces AttentionKernelOperator.matvec / matvec_impl
+ * (laker/kernels.py:187-270) and dense_attention_matvec (kernels.py:121-130)
+ * for float32 operators. */
+int laker_attn_matvec_f32(const float* rows32, int64_t m, const float* cols32, int64_t n, int d,
+                          float lam, int clamp, const float* X, int k, int64_t ldx, float* Y,
+                          int64_t ldy, void* workspace, size_t workspace_bytes, void* stream);
+
+/* FP64 fused matvec / residual ("accurate" operator: FP64 logits, FP64 exp,
+ * FP64 accumulation).
+ *   Y = B - (lam * X[:m] + exp(Er Ec^T) X)    if B != NULL
+ *   Y =      lam * X[:m] + exp(Er Ec^T) X     otherwise
+ * Er/Ec are packed64 buffers.  Used for the true-residual recomputation of
+ * the PCG loop and for float64 operators and predictions.
+ * Replaces the float64 path of AttentionKernelOperator.matvec
+ * (laker/kernels.py:187-270), the residual replacement r = b - A x
+ * (laker/solvers.py:264) and the exact-kernel prediction loop
+ * (laker/core.py:633-655). */
+int laker_attn_matvec_f64(const double* rows64, int64_t m, const double* cols64, int64_t n, int d,
+                          double lam, int clamp, const double* X, int k, int64_t ldx,
+                          const double* B, int64_t ldb, double* Y, int64_t ldy, void* workspace,
+                          size_t workspace_bytes, void* stream);
+
+/* diag(A) = lam + exp(||e_i||^2) in FP64.
+ * Replaces AttentionKernelOperator.diagonal (laker/kernels.py:272-283). */
+int laker_attn_diagonal(const double* packed64, int64_t n, int d, double lam, double* out,
+                        void* stream);
+
+/* Materialised kernel block K = exp(Er Ec^T) (m x p), FP32 or FP64 output
+ * (out_is_f64), computed from the packed64 embeddings with FP64 logits.
+ * Replaces AttentionKernelOperator.kernel_eval (laker/kernels.py:301-354). */
+int laker_kernel_eval(const double* rows64, int64_t m, const double* cols64, int64_t p, int d,
+                      int clamp, void* out, int out_is_f64, int64_t ldo, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Factored CCCP preconditioner                                              */
+/* ------------------------------------------------------------------------ */
+typedef struct laker_precond {
+  const float* q_basis; /* (n x nr) row-major, orthonormal columns Q          */
+  const float* w_core;  /* (nr x nr) row-major W = V diag(l^-1/2 - c^-1/2) V^T */
+  int64_t n;
+  int nr;
+  double inv_sqrt_iso; /* c^-1/2, c = isotropic coefficient                  */
+} laker_precond;
+
+size_t laker_precond_workspace_bytes(int64_t n, int nr, int k);
+
+/* Z = P R = c^-1/2 R + Q W Q^T R for R (n x k), FP64 in, FP32 or FP64 out.
+ * Replaces preconditioner_apply_core / CCCPPreconditioner.apply
+ * (laker/preconditioner.py:52-68, :286-310). */
+int laker_precond_apply(const laker_precond* pc, const double* R, int k, int64_t ldr, void* Z,
+                        int z_is_f64, int64_t ldz, void* workspace, size_t workspace_bytes,
+                        void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Preconditioned conjugate gradient                                         */
+/* ------------------------------------------------------------------------ */
+typedef struct laker_operator {
+  const float* packed32;  /* packed32 embeddings (sloppy FP32 operator)     */
+  const double* packed64; /* packed64 embeddings (accurate FP64 operator)   */
+  int64_t n;
+  int d;
+  double lambda_reg;
+  int clamp;
+} laker_operator;
+
+typedef struct laker_pcg_params {
+  double tol;            /* stop when ||b - A x||_F <= tol ||b||_F (FP64 A)  */
+  int max_iter;          /* iteration cap (reference default: n)           */
+  double reliable_delta; /* FP64 residual recomputed when the recurrence
+                            residual fell by this factor (default 0.1)      */
+  double breakdown_eps;  /* breakdown test p^T A p <= -eps ||p|| ||Ap||     */
+  int check_every;       /* host polls the device status every N iterations */
+  int has_x0;            /* 1: X holds the initial guess on entry           */
+} laker_pcg_params;
+
+typedef struct laker_pcg_result {
+  int status;              /* LAKER_OK / _BREAKDOWN / _NOT_CONVERGED / ...  */
+  int iterations;          /* PCG iterations (FP32 operator applications)   */
+  int accurate_matvecs;    /* FP64 residual recomputations                  */
+  double residual_norm;    /* ||b - A x||_F of the returned x (FP64 A)      */
+  double rhs_norm;         /* ||b||_F                                       */
+  double recurrence_norm;  /* last recurrence residual norm                 */
+} laker_pcg_result;
+
+size_t laker_pcg_workspace_bytes(int64_t n, int d, int nr, int k);
+
+/* Solves A X = B for B (n x k, row-major, ld = k) with mixed-precision PCG:
+ * FP32 fused operator inside the iteration, FP64 vectors, inner products and
+ * scalars on the device, and reliable updates that replace the recurrence
+ * residual by the FP64 residual B - A X.  k = 1 is the single-RHS solve;
+ * k > 1 uses column-wise alpha/beta and the global Frobenius stop test of the
+ * batched-RHS solve.  `pc` may be NULL (identity preconditioner).
+ * Replaces PreconditionedConjugateGradient.solve / solve_1d / solve_2d
+ * (laker/solvers.py:130-394). */
+int laker_pcg_solve(const laker_operator* op, const laker_precond* pc, const double* B, int k,
+                    double* X, const laker_pcg_params* params, void* workspace,
+                    size_t workspace_bytes, laker_pcg_result* result, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Predictive variance                                                       */
+/* ------------------------------------------------------------------------ */
+/* var_q = max(0, exp(||e_q||^2) - sum_i Kxq[i, q] * V[i, q]) for q < m, with
+ * Kxq, V (n x m) row-major FP64 and Eq the packed64 query embeddings.
+ * Replaces laker/core.py:754-758 and :777 without the m x m kernel_eval. */
+int laker_variance_finalize(const double* q64, int64_t m, int d, const double* Kxq,
+                            const double* V, int64_t n, int64_t ld, double* var, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Roofline denominators                                                     */
+/* ------------------------------------------------------------------------ */
+/* Measures, on the current device, the sustained FP32 FMA rate (TFLOP/s,
+ * 2 flops per FMA), the MUFU exp2 rate (Tops/s) and the FP64 FMA rate
+ * (TFLOP/s) with short register-resident microkernels (~50 ms).  `scratch`
+ * must hold laker_peaks_scratch_bytes() bytes. */
+size_t laker_peaks_scratch_bytes(void);
+int laker_measure_peaks(void* scratch, double* ffma_tflops, double* mufu_tops,
+                        double* dfma_tflops, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LAKER_B200_H */

@@ -1,0 +1,179 @@
+// Shared device helpers for the LAKER B200 solve path (sm_100a only).
+//
+// Everything here is header-only so that each translation unit of
+// liblaker_b200.so can inline it; no relocatable device code is needed.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/laker_b200.h"
+
+#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ < 1000)
+#error "liblaker_b200 targets sm_100a (B200) only"
+#endif
+
+namespace laker {
+
+// log2(e): the kernel entry exp(s) is evaluated as exp2(s * log2(e)), with
+// log2(e) folded into the row-side embedding once per CTA.
+constexpr float kLog2e = 1.4426950408889634f;
+
+// The reference clamps the Gram entry at 80 (float32) before exp when
+// max ||e_i||^2 >= 80 (laker/kernels.py:98-107, :181-185).  In the exp2
+// domain that is 80 * log2(e).
+constexpr float kClampLog2 = 80.0f * 1.4426950408889634f;
+constexpr double kClamp64 = 700.0;
+
+// Columns staged per shared-memory tile by the FP32 and FP64 matvecs.
+constexpr int kTileCols32 = 256;  // 128 column pairs
+constexpr int kTileCols64 = 128;
+
+__host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+__host__ __device__ inline int64_t round_up(int64_t a, int64_t b) { return ceil_div(a, b) * b; }
+
+// Embedding dimension padded to an even count: the FP32 layout interleaves
+// point pairs (see pack.cu), and every pair block must be 16-byte aligned.
+__host__ __device__ inline int padded_dim(int d) { return (d + 1) & ~1; }
+
+// Number of point pairs stored by the packed FP32 layout for n points: enough
+// whole column tiles that every TMA bulk copy of a tile stays in bounds.
+__host__ __device__ inline int64_t packed_pairs(int64_t n) {
+  return round_up(ceil_div(n, 2) > 0 ? ceil_div(n, 2) : 1, kTileCols32 / 2);
+}
+// Number of rows stored by the packed FP64 layout.
+__host__ __device__ inline int64_t packed_rows64(int64_t n) {
+  return round_up(n > 0 ? n : 1, kTileCols64);
+}
+
+// ---------------------------------------------------------------------------
+// Device status word.  Kernels never trap: a failed bounded wait records an
+// error code here and the CTA returns; the host reads the word after the
+// stream synchronises.
+// ---------------------------------------------------------------------------
+__device__ inline void record_status(int* status, int code) {
+  if (status) atomicCAS(status, 0, code);
+}
+
+// ---------------------------------------------------------------------------
+// Fast exp2 on the MUFU pipe (PTX ex2.approx, flush-to-zero).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// ---------------------------------------------------------------------------
+// mbarrier + 1-D TMA bulk copy (cp.async.bulk) wrappers.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+// Bulk global->shared copy completing on `bar`.  dst, src and bytes must be
+// multiples of 16 (guaranteed by the packed layouts).
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_timer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait on an mbarrier phase.  Returns false (and records
+// LAKER_ERR_TIMEOUT) if the phase did not complete within ~2 s.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* status) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_timer_ns();
+  for (uint32_t it = 0; it < (1u << 30); ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 255u) == 0 && global_timer_ns() - t0 > 2000000000ull) break;
+  }
+  record_status(status, LAKER_ERR_TIMEOUT);
+  return false;
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic block reductions (fixed shuffle tree + fixed warp order).
+// ---------------------------------------------------------------------------
+template <typename V>
+__device__ __forceinline__ V warp_sum(V v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Sums NV values over the block; result valid in every thread of warp 0.
+// `scratch` must hold NV * (T/32) doubles.
+template <int T, int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double* scratch) {
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) v[q] = warp_sum(v[q]);
+  if (l == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) scratch[q * (T / 32) + w] = v[q];
+  }
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+      double t = (l < T / 32) ? scratch[q * (T / 32) + l] : 0.0;
+      v[q] = warp_sum(t);
+    }
+  }
+  __syncthreads();
+}
+
+// Grid completion detector for "last block finishes the reduction": every
+// block publishes its partials, then calls this; exactly one block (the last
+// to arrive) gets true.  The counter is reset by that block for reuse.
+__device__ __forceinline__ bool arrive_last_block(unsigned int* counter) {
+  __shared__ bool s_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned int total = gridDim.x * gridDim.y * gridDim.z;
+    const unsigned int t = atomicAdd(counter, 1u);
+    s_last = (t == total - 1);
+    if (s_last) *counter = 0;  // every block has arrived; safe to rearm
+  }
+  __syncthreads();
+  if (s_last) __threadfence();
+  return s_last;
+}
+
+}  // namespace laker

@@ -1,0 +1,55 @@
+// Host-side launchers shared between the translation units of liblaker_b200.
+#pragma once
+
+#include "common.cuh"
+
+namespace laker {
+
+// Every caller-provided workspace starts with this header; `status` receives
+// device-side failures (LAKER_ERR_TIMEOUT) of the kernels launched with it.
+struct alignas(256) WsHeader {
+  int status;
+  int pad[63];
+};
+constexpr size_t kWsHeader = sizeof(WsHeader);
+
+// Records a CUDA failure for laker_last_cuda_error() and returns LAKER_ERR_CUDA.
+int fail_cuda(cudaError_t e);
+
+// Streaming multiprocessor count of the current device (cached per device).
+int sm_count();
+
+// Split of the column range into S segments of cols_per_seg columns (a
+// multiple of the staging tile) so that row blocks x segments fill whole
+// waves of CTAs.
+struct SegPlan {
+  int S;
+  int64_t cols_per_seg;
+};
+SegPlan plan_segments(int64_t m, int64_t n, int rows_per_cta, int ctas_per_sm, int tile);
+
+// ---- single-RHS fused matvecs: write per-segment FP64 row partials --------
+// part[s * m + i] = sum_{j in segment s} exp(er_i . ec_j) x_j
+SegPlan k1_plan(int64_t m, int64_t n, int d);
+cudaError_t launch_k1(const float* rows32, int64_t m, const float* cols32, int64_t n, int d,
+                      int clamp, const float* x, double* part, const SegPlan& plan, int* status,
+                      const int* gate, cudaStream_t s);
+
+SegPlan k4_plan(int64_t m, int64_t n, int d);
+cudaError_t launch_k4(const double* rows64, int64_t m, const double* cols64, int64_t n, int d,
+                      int clamp, const double* x, double* part, const SegPlan& plan, int* status,
+                      const int* gate, cudaStream_t s);
+
+// `gate` (nullable): the kernel does nothing when *gate == 0.
+
+// ---- multi-RHS fused matvecs (CUDA cores) ----------------------------------
+// Y[i, :] = lam * X[i, :] (if m == n) + sum_j exp(er_i . ec_j) X[j, :]
+cudaError_t launch_multi_f32(const float* rows32, int64_t m, const float* cols32, int64_t n, int d,
+                             float lam, int clamp, const float* X, int k, int64_t ldx, float* Y,
+                             int64_t ldy, cudaStream_t s);
+// Y = B - (lam X + K X) when B != nullptr, else lam X + K X (FP64 throughout).
+cudaError_t launch_multi_f64(const double* rows64, int64_t m, const double* cols64, int64_t n, int d,
+                             double lam, int clamp, const double* X, int k, int64_t ldx,
+                             const double* B, int64_t ldb, double* Y, int64_t ldy, cudaStream_t s);
+
+}  // namespace laker

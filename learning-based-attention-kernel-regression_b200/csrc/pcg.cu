@@ -1,0 +1,410 @@
+// Mixed-precision preconditioned conjugate gradient, device resident.
+//
+// Iteration (single RHS), all scalars on the device:
+//   part = K32 p                         FP32 fused matvec (K1), FP64 partials
+//   Ap = lam p + sum(part); p.Ap, |p|, |Ap|      -> alpha, breakdown test
+//   x += alpha p; r -= alpha Ap; |r|             (x, r in FP64)
+//   if |r| <= delta |r_last_true| or |r| <= tol |b| or iter == max_iter:
+//       r = b - A64 x                    FP64 fused residual (K4), |r|
+//       converged when |r| <= tol |b|
+//   u = Q^T r; v = W u; z = c^-1/2 r + Q v; r.z   -> beta
+//   p = z + beta p
+// The recurrence follows solve_1d (laker/solvers.py:189-295); the reliable
+// update (FP64 residual replacement) is what lets an FP32 operator reach the
+// float64 reference's residual: the stop test is always taken on the FP64
+// residual.  Every kernel reads the device state first and does nothing once
+// the solve has finished, so the host can launch several iterations between
+// status polls.
+#include "pcg_state.cuh"
+
+namespace laker {
+int precond_grid();
+
+namespace {
+
+constexpr int T = kVecThreads;
+
+int vec_grid(int64_t n) {
+  int64_t g = ceil_div(n, T * 4);
+  const int64_t cap = 2 * (int64_t)sm_count();
+  if (g > cap) g = cap;
+  return (int)(g < 1 ? 1 : g);
+}
+
+// x = 0 (unless warm start), r = b, |b| -> bnorm, tol_abs, rmax.
+__global__ void __launch_bounds__(T)
+    pcg_init_kernel(const double* __restrict__ b, double* __restrict__ x, double* __restrict__ r,
+                    int64_t n, int has_x0, double tol, double* blockpart, PcgState* st) {
+  __shared__ double s_red[T / 32];
+  double acc = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)T + threadIdx.x; i < n; i += (int64_t)gridDim.x * T) {
+    const double bi = b[i];
+    r[i] = bi;
+    if (!has_x0) x[i] = 0.0;
+    acc = fma(bi, bi, acc);
+  }
+  double v[1] = {acc};
+  block_sum<T, 1>(v, s_red);
+  if (threadIdx.x == 0) blockpart[blockIdx.x] = v[0];
+  if (!arrive_last_block(&st->counters[kCtrBnorm])) return;
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (unsigned int k = 0; k < gridDim.x; ++k) t += __ldcg(blockpart + k);
+    const double bn = sqrt(t);
+    st->bnorm = bn;
+    st->tol_abs = tol * bn;
+    st->rnorm = bn;
+    st->rmax = bn;
+    st->true_rnorm = bn;
+    if (!isfinite(bn)) {
+      st->status = LAKER_ERR_NONFINITE;
+      st->done = 1;
+      st->active = 0;
+    }
+  }
+}
+
+// Ap = lam p + sum_s part[s]; p.Ap, p.p, Ap.Ap -> breakdown test and alpha.
+__global__ void __launch_bounds__(T)
+    pcg_after_matvec_kernel(const double* __restrict__ part, int S, const float* __restrict__ p,
+                            float* __restrict__ Ap, int64_t n, double* blockpart, PcgState* st) {
+  if (st->done) return;
+  __shared__ double s_red[3 * (T / 32)];
+  const double lam = st->lam;
+  double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)T + threadIdx.x; i < n; i += (int64_t)gridDim.x * T) {
+    const double pi = p[i];
+    double a = lam * pi;
+    for (int s = 0; s < S; ++s) a += part[(int64_t)s * n + i];
+    const float af = (float)a;
+    Ap[i] = af;
+    d0 = fma(pi, (double)af, d0);
+    d1 = fma(pi, pi, d1);
+    d2 = fma((double)af, (double)af, d2);
+  }
+  double v[3] = {d0, d1, d2};
+  block_sum<T, 3>(v, s_red);
+  if (threadIdx.x == 0) {
+    blockpart[3 * blockIdx.x + 0] = v[0];
+    blockpart[3 * blockIdx.x + 1] = v[1];
+    blockpart[3 * blockIdx.x + 2] = v[2];
+  }
+  if (!arrive_last_block(&st->counters[kCtrMatvec])) return;
+  if (threadIdx.x == 0) {
+    double pap = 0.0, pp = 0.0, aa = 0.0;
+    for (unsigned int k = 0; k < gridDim.x; ++k) {
+      pap += __ldcg(blockpart + 3 * k + 0);
+      pp += __ldcg(blockpart + 3 * k + 1);
+      aa += __ldcg(blockpart + 3 * k + 2);
+    }
+    st->pAp = pap;
+    if (!isfinite(pap) || !isfinite(pp) || !isfinite(aa)) {
+      st->status = LAKER_ERR_NONFINITE;
+      st->done = 1;
+      st->active = 0;
+    } else if (pap <= -st->eps * sqrt(pp) * sqrt(aa)) {
+      // non-positive curvature (laker/solvers.py:232-246)
+      st->status = LAKER_ERR_BREAKDOWN;
+      st->done = 1;
+      st->active = 0;
+    } else {
+      st->alpha = st->rz / pap;
+    }
+  }
+}
+
+// x += alpha p; r -= alpha Ap; |r| -> decide on the FP64 recomputation.
+__global__ void __launch_bounds__(T)
+    pcg_update_xr_kernel(const float* __restrict__ p, const float* __restrict__ Ap,
+                         double* __restrict__ x, double* __restrict__ r, int64_t n,
+                         double* blockpart, PcgState* st) {
+  if (st->done) return;
+  __shared__ double s_red[T / 32];
+  const double alpha = st->alpha;
+  double acc = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)T + threadIdx.x; i < n; i += (int64_t)gridDim.x * T) {
+    x[i] = fma(alpha, (double)p[i], x[i]);
+    const double ri = fma(-alpha, (double)Ap[i], r[i]);
+    r[i] = ri;
+    acc = fma(ri, ri, acc);
+  }
+  double v[1] = {acc};
+  block_sum<T, 1>(v, s_red);
+  if (threadIdx.x == 0) blockpart[blockIdx.x] = v[0];
+  if (!arrive_last_block(&st->counters[kCtrUpdate])) return;
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (unsigned int k = 0; k < gridDim.x; ++k) t += __ldcg(blockpart + k);
+    const double rn = sqrt(t);
+    st->rnorm = rn;
+    st->iter += 1;
+    st->need_update =
+        (rn <= st->delta * st->rmax || rn <= st->tol_abs || st->iter >= st->max_iter || !isfinite(rn))
+            ? 1
+            : 0;
+  }
+}
+
+// After the FP64 matvec: r = b - (lam x + sum_s part[s]), |r| -> stop test.
+// `init` seeds the state for a warm start (no iteration has run yet).
+__global__ void __launch_bounds__(T)
+    pcg_after_residual_kernel(const double* __restrict__ part, int S, const double* __restrict__ b,
+                              const double* __restrict__ x, double* __restrict__ r, int64_t n,
+                              int init, double* blockpart, PcgState* st) {
+  if (st->done || (!init && !st->need_update)) return;
+  __shared__ double s_red[T / 32];
+  const double lam = st->lam;
+  double acc = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)T + threadIdx.x; i < n; i += (int64_t)gridDim.x * T) {
+    double a = lam * x[i];
+    for (int s = 0; s < S; ++s) a += part[(int64_t)s * n + i];
+    const double ri = b[i] - a;
+    r[i] = ri;
+    acc = fma(ri, ri, acc);
+  }
+  double v[1] = {acc};
+  block_sum<T, 1>(v, s_red);
+  if (threadIdx.x == 0) blockpart[blockIdx.x] = v[0];
+  if (!arrive_last_block(&st->counters[kCtrResid])) return;
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (unsigned int k = 0; k < gridDim.x; ++k) t += __ldcg(blockpart + k);
+    const double rn = sqrt(t);
+    st->rnorm = rn;
+    st->true_rnorm = rn;
+    st->rmax = rn;
+    st->n_accurate += 1;
+    st->need_update = 0;
+    if (!isfinite(rn)) {
+      st->status = LAKER_ERR_NONFINITE;
+      st->done = 1;
+      st->active = 0;
+    } else if (!init && rn <= st->tol_abs) {
+      st->status = LAKER_OK;
+      st->done = 1;
+      st->active = 0;
+    } else if (!init && st->iter >= st->max_iter) {
+      st->status = LAKER_ERR_NOT_CONVERGED;
+      st->done = 1;
+      st->active = 0;
+    }
+  }
+}
+
+// p = z + beta p; on the first call (init) p = z, without reading the
+// uninitialised p.
+__global__ void __launch_bounds__(T)
+    pcg_update_p_kernel(const float* __restrict__ z, float* __restrict__ p, int64_t n,
+                        const PcgState* st, int init) {
+  if (st->done) return;
+  const float beta = (float)st->beta;
+  for (int64_t i = blockIdx.x * (int64_t)T + threadIdx.x; i < n; i += (int64_t)gridDim.x * T)
+    p[i] = init ? z[i] : fmaf(beta, p[i], z[i]);
+}
+
+// Identity preconditioner: z = r, and r.z folded into beta like the fused apply.
+__global__ void __launch_bounds__(T)
+    identity_expand_kernel(const double* __restrict__ r, float* __restrict__ z, int64_t n,
+                           double* blockpart, PcgState* st, int init) {
+  if (st->done) return;
+  __shared__ double s_red[T / 32];
+  double acc = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)T + threadIdx.x; i < n; i += (int64_t)gridDim.x * T) {
+    const float zi = (float)r[i];
+    z[i] = zi;
+    acc = fma(r[i], (double)zi, acc);
+  }
+  double v[1] = {acc};
+  block_sum<T, 1>(v, s_red);
+  if (threadIdx.x == 0) blockpart[blockIdx.x] = v[0];
+  if (!arrive_last_block(&st->counters[kCtrExpand])) return;
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (unsigned int k = 0; k < gridDim.x; ++k) t += __ldcg(blockpart + k);
+    if (init) {
+      st->rz = t;
+      st->beta = 0.0;
+    } else {
+      st->beta = t / st->rz;
+      st->rz = t;
+    }
+  }
+}
+
+// Workspace carve-up of one single-RHS solve.
+struct PcgWs {
+  WsHeader* hdr;
+  PcgState* st;
+  double* r;
+  float* Ap;
+  float* z;
+  float* p;
+  double* part32;  // S1 x n FP64 partials of the FP32 matvec
+  double* part64;  // S4 x n FP64 partials of the FP64 matvec
+  double* blockpart;
+  double* upart;
+  double* v;
+  size_t bytes;
+};
+
+PcgWs carve(void* base, int64_t n, int d, int nr) {
+  PcgWs w{};
+  char* p = static_cast<char*>(base);
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    char* q = p ? p + off : nullptr;
+    off += (size_t)round_up((int64_t)bytes, 256);
+    return q;
+  };
+  const SegPlan p1 = k1_plan(n, n, d), p4 = k4_plan(n, n, d);
+  const int G = vec_grid(n) > precond_grid() ? vec_grid(n) : precond_grid();
+  w.hdr = reinterpret_cast<WsHeader*>(take(kWsHeader));
+  w.st = reinterpret_cast<PcgState*>(take(sizeof(PcgState)));
+  w.r = reinterpret_cast<double*>(take(n * sizeof(double)));
+  w.Ap = reinterpret_cast<float*>(take(n * sizeof(float)));
+  w.z = reinterpret_cast<float*>(take(n * sizeof(float)));
+  w.p = reinterpret_cast<float*>(take(n * sizeof(float)));
+  w.part32 = reinterpret_cast<double*>(take((size_t)p1.S * n * sizeof(double)));
+  w.part64 = reinterpret_cast<double*>(take((size_t)p4.S * n * sizeof(double)));
+  w.blockpart = reinterpret_cast<double*>(take((size_t)G * 4 * sizeof(double)));
+  w.upart = reinterpret_cast<double*>(take((size_t)precond_grid() * (nr > 0 ? nr : 1) * sizeof(double)));
+  w.v = reinterpret_cast<double*>(take((size_t)(nr > 0 ? nr : 1) * sizeof(double)));
+  w.bytes = off;
+  return w;
+}
+
+}  // namespace
+}  // namespace laker
+
+using namespace laker;
+
+extern "C" size_t laker_pcg_workspace_bytes(int64_t n, int d, int nr, int k) {
+  if (n < 1 || d < 1 || d > 16 || nr < 0 || nr > kMaxNr || k < 1) return 0;
+  if (k != 1) return 0;
+  return carve(nullptr, n, d, nr).bytes;
+}
+
+extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc, const double* B,
+                               int k, double* X, const laker_pcg_params* prm, void* workspace,
+                               size_t workspace_bytes, laker_pcg_result* res, void* stream) {
+  if (!op || !prm || !res || !B || !X || !workspace) return LAKER_ERR_INVALID_ARG;
+  if (op->n < 1 || op->d < 1 || op->d > 16 || !op->packed32 || !op->packed64) return LAKER_ERR_INVALID_ARG;
+  if (k != 1) return LAKER_ERR_UNSUPPORTED;
+  if (pc && (pc->n != op->n || pc->nr < 1 || pc->nr > kMaxNr || !pc->q_basis || !pc->w_core))
+    return LAKER_ERR_INVALID_ARG;
+  if (prm->max_iter < 0 || !(prm->tol >= 0.0) || !(prm->reliable_delta > 0.0)) return LAKER_ERR_INVALID_ARG;
+  const int64_t n = op->n;
+  const int d = op->d;
+  const int nr = pc ? pc->nr : 0;
+  if (workspace_bytes < laker_pcg_workspace_bytes(n, d, nr, k)) return LAKER_ERR_WORKSPACE;
+
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  PcgWs w = carve(workspace, n, d, nr);
+  const SegPlan p1 = k1_plan(n, n, d), p4 = k4_plan(n, n, d);
+  const int G = vec_grid(n), Gp = precond_grid();
+  const PcView view{pc ? pc->q_basis : nullptr, pc ? pc->w_core : nullptr, n, nr,
+                    pc ? pc->inv_sqrt_iso : 1.0};
+
+  *res = laker_pcg_result{};
+  PcgState h{};
+  h.delta = prm->reliable_delta;
+  h.eps = prm->breakdown_eps;
+  h.lam = op->lambda_reg;
+  h.max_iter = prm->max_iter;
+  h.active = 1;
+  cudaError_t e = cudaMemsetAsync(w.hdr, 0, kWsHeader, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(w.st, &h, sizeof(PcgState), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return fail_cuda(e);
+
+  int* dstatus = &w.hdr->status;
+  auto launch_precond = [&](int init) {
+    if (pc) {
+      pc_project_kernel<T><<<Gp, T, 0, s>>>(view, w.r, w.upart, w.v, &w.st->counters[kCtrProject],
+                                           &w.st->active);
+      pc_expand_kernel<T, float><<<Gp, T, 0, s>>>(view, w.r, w.v, w.z, w.blockpart,
+                                                 &w.st->counters[kCtrExpand], w.st, init, nullptr,
+                                                 &w.st->active);
+    } else {
+      identity_expand_kernel<<<G, T, 0, s>>>(w.r, w.z, n, w.blockpart, w.st, init);
+    }
+    pcg_update_p_kernel<<<G, T, 0, s>>>(w.z, w.p, n, w.st, init);
+  };
+
+  // ---- initialisation ------------------------------------------------------
+  pcg_init_kernel<<<G, T, 0, s>>>(B, X, w.r, n, prm->has_x0, prm->tol, w.blockpart, w.st);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return fail_cuda(e);
+  if (prm->has_x0) {
+    // warm start: r = b - A x0 with the FP64 operator (laker/solvers.py:165-173)
+    e = launch_k4(op->packed64, n, op->packed64, n, d, op->clamp, X, w.part64, p4, dstatus, nullptr, s);
+    if (e != cudaSuccess) return fail_cuda(e);
+    pcg_after_residual_kernel<<<G, T, 0, s>>>(w.part64, p4.S, B, X, w.r, n, 1, w.blockpart, w.st);
+  }
+  e = cudaMemcpyAsync(&h, w.st, sizeof(PcgState), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fail_cuda(e);
+  res->rhs_norm = h.bnorm;
+  if (h.bnorm == 0.0) {
+    // zero right-hand side: x is returned unchanged (zero, or x0), as in
+    // laker/solvers.py:177-182
+    res->status = LAKER_OK;
+    res->residual_norm = 0.0;
+    return LAKER_OK;
+  }
+  if (h.done) {
+    res->status = h.status;
+    res->residual_norm = h.true_rnorm;
+    return h.status;
+  }
+  launch_precond(1);
+
+  // ---- iterations ----------------------------------------------------------
+  int check = prm->check_every;
+  if (check < 1) {
+    // poll roughly every 10 ms of FP32 operator work (~2e12 entries/s)
+    const double est_s = (double)n * (double)n / 2e12 + 40e-6;
+    check = (int)(0.01 / est_s);
+    if (check < 1) check = 1;
+    if (check > 64) check = 64;
+  }
+  int launched = 0;
+  while (launched < prm->max_iter) {
+    const int chunk = (prm->max_iter - launched) < check ? (prm->max_iter - launched) : check;
+    for (int c = 0; c < chunk; ++c) {
+      launch_k1(op->packed32, n, op->packed32, n, d, op->clamp, w.p, w.part32, p1, dstatus,
+                &w.st->active, s);
+      pcg_after_matvec_kernel<<<G, T, 0, s>>>(w.part32, p1.S, w.p, w.Ap, n, w.blockpart, w.st);
+      pcg_update_xr_kernel<<<G, T, 0, s>>>(w.p, w.Ap, X, w.r, n, w.blockpart, w.st);
+      launch_k4(op->packed64, n, op->packed64, n, d, op->clamp, X, w.part64, p4, dstatus,
+                &w.st->need_update, s);
+      pcg_after_residual_kernel<<<G, T, 0, s>>>(w.part64, p4.S, B, X, w.r, n, 0, w.blockpart, w.st);
+      launch_precond(0);
+    }
+    launched += chunk;
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, w.st, sizeof(PcgState), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail_cuda(e);
+    if (h.done) break;
+  }
+
+  int dev_status = 0;
+  e = cudaMemcpy(&dev_status, dstatus, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return fail_cuda(e);
+  res->iterations = h.iter;
+  res->accurate_matvecs = h.n_accurate;
+  res->residual_norm = h.true_rnorm;
+  res->recurrence_norm = h.rnorm;
+  res->rhs_norm = h.bnorm;
+  if (dev_status != 0) {
+    res->status = dev_status;
+    return dev_status;
+  }
+  if (!h.done) {
+    // max_iter == 0: nothing ran
+    res->status = LAKER_ERR_NOT_CONVERGED;
+    return LAKER_ERR_NOT_CONVERGED;
+  }
+  res->status = h.status;
+  return h.status;
+}

@@ -1,0 +1,199 @@
+"""Exact attention-kernel operator on the B200 kernels.
+
+Drop-in for laker.kernels.AttentionKernelOperator (laker/kernels.py:133-354):
+same constructor, attributes (n, embedding_dim, lambda_reg, chunk_size,
+device, dtype, embeddings, shape, skip_clamp) and methods (matvec, diagonal,
+to_dense, kernel_eval).  The operator is applied by fused CUDA kernels that
+never store the n x n kernel: float32 operators use the FP32 flash-style
+matvec, float64 operators the FP64 one.  `chunk_size` is accepted and kept for
+API compatibility; the fused kernels tile on chip and need no memory budget.
+"""
+
+from __future__ import annotations
+
+import logging
+from typing import Optional, Protocol, Tuple
+
+import torch
+
+from . import _lib
+
+logger = logging.getLogger(__name__)
+
+MAX_EMBEDDING_DIM = 16
+
+
+class KernelOperator(Protocol):
+    """Protocol for matrix-free kernel operators (laker/kernels.py:43-72)."""
+
+    n: int
+    embedding_dim: int
+    lambda_reg: float
+    dtype: torch.dtype
+    device: torch.device
+    shape: Tuple[int, int]
+
+    def matvec(self, x: torch.Tensor) -> torch.Tensor: ...
+
+    def diagonal(self) -> torch.Tensor: ...
+
+    def to_dense(self) -> torch.Tensor: ...
+
+    def kernel_eval(
+        self, x: torch.Tensor, y: Optional[torch.Tensor] = None, chunk_size: Optional[int] = None
+    ) -> torch.Tensor: ...
+
+
+def _safe_limit(dtype: torch.dtype) -> float:
+    # exp_safe clamp level (laker/kernels.py:98-99)
+    return 80.0 if dtype == torch.float32 else 700.0
+
+
+class PackedEmbeddings:
+    """Device copies of an embedding matrix in the two kernel layouts."""
+
+    def __init__(self, E: torch.Tensor) -> None:
+        _lib.require_cuda(E, "embeddings")
+        if E.dim() != 2:
+            raise ValueError(f"embeddings must be 2-D, got shape {tuple(E.shape)}")
+        if not 1 <= E.shape[1] <= MAX_EMBEDDING_DIM:
+            raise ValueError(
+                f"embedding_dim must be in [1, {MAX_EMBEDDING_DIM}] for the fused kernels, "
+                f"got {E.shape[1]}"
+            )
+        self.n, self.d = int(E.shape[0]), int(E.shape[1])
+        self.packed32 = _lib.pack_f32(E.detach())
+        self.packed64 = _lib.pack_f64(E.detach())
+
+
+class AttentionKernelOperator:
+    """Matrix-free operator A = lambda*I + exp(E E^T) on the GPU.
+
+    Args:
+        embeddings: (n, embedding_dim) tensor on a CUDA device, embedding_dim <= 16.
+        lambda_reg: Tikhonov regularisation lambda.
+        chunk_size: accepted for compatibility (unused by the fused kernels).
+        device / dtype: default to the embeddings' own.
+
+    Raises:
+        ValueError: if embeddings is not 2-D.
+        RuntimeError: if the device is not CUDA.
+    """
+
+    def __init__(
+        self,
+        embeddings: torch.Tensor,
+        lambda_reg: float = 1e-2,
+        chunk_size: Optional[int] = None,
+        device: Optional[torch.device] = None,
+        dtype: Optional[torch.dtype] = None,
+    ) -> None:
+        if embeddings.dim() != 2:
+            raise ValueError(f"embeddings must be 2-D, got shape {embeddings.shape}")
+        self.n = embeddings.shape[0]
+        self.embedding_dim = embeddings.shape[1]
+        self.lambda_reg = float(lambda_reg)
+        self.chunk_size = chunk_size
+        if device is None:
+            device = embeddings.device
+        if dtype is None:
+            dtype = embeddings.dtype
+        self.device = torch.device(device)
+        self.dtype = dtype
+        self.embeddings = embeddings.to(device=self.device, dtype=dtype)
+        _lib.require_cuda(self.embeddings, "embeddings")
+        self.shape = (self.n, self.n)
+        self._packed = PackedEmbeddings(self.embeddings)
+        max_sq_norm = torch.sum(self.embeddings.detach() ** 2, dim=1).max().item() if self.n else 0.0
+        self.skip_clamp = max_sq_norm < _safe_limit(self.dtype)
+
+    # -- device-level handles used by the fused solver ---------------------
+    @property
+    def packed(self) -> PackedEmbeddings:
+        return self._packed
+
+    def c_operator(self) -> _lib.laker_operator:
+        return _lib.laker_operator(
+            self._packed.packed32.data_ptr(),
+            self._packed.packed64.data_ptr(),
+            self.n,
+            self.embedding_dim,
+            self.lambda_reg,
+            0 if self.skip_clamp else 1,
+        )
+
+    def _check_grad(self) -> None:
+        if self.embeddings.requires_grad and torch.is_grad_enabled():
+            raise NotImplementedError(
+                "autograd through the fused attention-kernel operator is not implemented"
+            )
+
+    # -- KernelOperator protocol ---------------------------------------------
+    def matvec(self, x: torch.Tensor) -> torch.Tensor:
+        """Apply (lambda I + G) to x of shape (n,) or (n, k)."""
+        if x.dim() not in (1, 2):
+            raise ValueError(f"x must be 1-D or 2-D, got shape {x.shape}")
+        if x.shape[0] != self.n:
+            raise ValueError(f"x has {x.shape[0]} rows, operator has n={self.n}")
+        self._check_grad()
+        _lib.require_cuda(x, "x")
+        if self.n == 0:
+            return torch.zeros_like(x)
+        clamp = 0 if self.skip_clamp else 1
+        p = self._packed
+        if self.dtype == torch.float64:
+            y = _lib.attn_matvec_f64(p.packed64, self.n, p.packed64, self.n, self.embedding_dim,
+                                     self.lambda_reg, clamp, x.to(torch.float64))
+        else:
+            y = _lib.attn_matvec_f32(p.packed32, self.n, p.packed32, self.n, self.embedding_dim,
+                                     self.lambda_reg, clamp, x.to(torch.float32))
+        return y.to(x.dtype) if x.dtype in (torch.float32, torch.float64) else y
+
+    def matvec_f64(self, x: torch.Tensor) -> torch.Tensor:
+        """FP64 (accurate) application regardless of the operator dtype."""
+        _lib.require_cuda(x, "x")
+        p = self._packed
+        return _lib.attn_matvec_f64(p.packed64, self.n, p.packed64, self.n, self.embedding_dim,
+                                    self.lambda_reg, 0 if self.skip_clamp else 1,
+                                    x.to(torch.float64))
+
+    def residual_f64(self, x: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
+        """b - A x with the FP64 operator."""
+        _lib.require_cuda(x, "x")
+        p = self._packed
+        return _lib.attn_matvec_f64(p.packed64, self.n, p.packed64, self.n, self.embedding_dim,
+                                    self.lambda_reg, 0 if self.skip_clamp else 1,
+                                    x.to(torch.float64), B=b.to(torch.float64))
+
+    def diagonal(self) -> torch.Tensor:
+        """diag(lambda I + G) = lambda + exp(||e_i||^2)."""
+        d = _lib.attn_diagonal(self._packed.packed64, self.n, self.embedding_dim, self.lambda_reg,
+                               self.device)
+        return d.to(self.dtype)
+
+    def to_dense(self) -> torch.Tensor:
+        """Materialise lambda I + G (O(n^2) memory: small n only)."""
+        p = self._packed
+        g = _lib.kernel_eval(p.packed64, self.n, p.packed64, self.n, self.embedding_dim, 0,
+                             self.dtype, self.device)
+        g.diagonal().add_(self.lambda_reg)
+        return g
+
+    def kernel_eval(
+        self, x: torch.Tensor, y: Optional[torch.Tensor] = None, chunk_size: Optional[int] = None
+    ) -> torch.Tensor:
+        """exp(x y^T) for x (m, d) and y (p, d) (y defaults to the embeddings)."""
+        del chunk_size  # the kernel tiles on chip
+        if x.dim() != 2:
+            raise ValueError(f"x must be 2-D, got shape {x.shape}")
+        _lib.require_cuda(x, "x")
+        if y is None:
+            cols64, p = self._packed.packed64, self.n
+        else:
+            if y.dim() != 2 or y.shape[1] != x.shape[1]:
+                raise ValueError(f"y must be 2-D with {x.shape[1]} columns, got {tuple(y.shape)}")
+            _lib.require_cuda(y, "y")
+            cols64, p = _lib.pack_f64(y.to(self.dtype)), y.shape[0]
+        rows64 = _lib.pack_f64(x.to(self.dtype))
+        return _lib.kernel_eval(rows64, x.shape[0], cols64, p, x.shape[1],
+                                0 if self.skip_clamp else 1, self.dtype, self.device)
