@@ -1,0 +1,504 @@
+#!/usr/bin/env python
+"""LAKER B200 solve-path benchmark.
+
+Workload (one "step"): one exact-kernel PCG solve of (lambda I + exp(E E^T)) a = y
+at n = 100,000 on the synthetic path-loss field (seed = rank), d = 10
+PositionEmbedding outputs, CCCP preconditioner with N_r = 256 probes built
+beforehand, tol 1e-6 on the TRUE relative residual (FP64 operator).  Inputs
+are resident in HBM for `value`; `e2e` repeats the solve through the public
+Python API with y copied from pinned host memory and alpha read back.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: one process per GPU under torchrun; every rank solves its own
+instance (replicas, weak scaling); timing is the max over ranks.
+`--impl reference` times the float64 CPU oracle of the reference path on the
+host cores (bounded sample, extrapolated) and prints the same JSON line.
+"""
+
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+METRIC = "PCG solves/sec & kernel entries/sec at n=100k @1e-6 resid; p50/p99 solve latency"
+N_DEFAULT = 100_000
+EMBED_DIM = 10
+NUM_PROBES = 256
+LAMBDA = 1e-2
+TOL = 1e-6
+MAX_ITER = 1000
+
+# Iterations the float64 reference recurrence (solve_1d, laker/solvers.py:189-295)
+# needs on the n=100,000 seed-0 system with the same CCCP preconditioner,
+# counted with `python bench.py --count-reference-iterations` on a B200 (the
+# float64 fused matvec applies the operator, the recurrence runs in numpy).
+# Used to extrapolate the bounded CPU samples to one full solve.
+REFERENCE_ITERATIONS = {100_000: 306}  # true relres 6.29e-7 at stop
+REFERENCE_ITERATIONS_FALLBACK = 300
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+def dist_info():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """Samples SM clock and clock-event reasons every 100 ms (NVML)."""
+
+    REASONS = {
+        0x4: "sw_power_cap",
+        0x8: "hw_slowdown",
+        0x20: "sw_thermal_slowdown",
+        0x40: "hw_thermal_slowdown",
+        0x80: "hw_power_brake_slowdown",
+    }
+
+    def __init__(self, device: torch.device) -> None:
+        self.samples = []
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._thread = None
+        self._nvml = None
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            handle = None
+            try:
+                uuid = str(torch.cuda.get_device_properties(device).uuid)
+                handle = pynvml.nvmlDeviceGetHandleByUUID(
+                    uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            except Exception:
+                handle = pynvml.nvmlDeviceGetHandleByIndex(device.index or 0)
+            self._nvml = pynvml
+            self._h = handle
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(handle, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self._nvml = None
+
+    def _reasons(self):
+        f = getattr(self._nvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or getattr(
+            self._nvml, "nvmlDeviceGetCurrentClocksThrottleReasons")
+        return int(f(self._h))
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                mhz = self._nvml.nvmlDeviceGetClockInfo(self._h, self._nvml.NVML_CLOCK_SM)
+                util = self._nvml.nvmlDeviceGetUtilizationRates(self._h).gpu
+                self.samples.append((mhz, self._reasons(), util))
+            except Exception:
+                pass
+            self._stop.wait(0.1)
+
+    def start(self):
+        if self._nvml is not None:
+            self._thread = threading.Thread(target=self._run, daemon=True)
+            self._thread.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._thread is not None:
+            self._thread.join()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": [], "samples": 0}
+        loaded = [s for s in self.samples if s[2] > 50] or self.samples
+        reasons = set()
+        for _, bits, _ in self.samples:
+            for bit, name in self.REASONS.items():
+                if bits & bit:
+                    reasons.add(name)
+        return {
+            "sm_mhz": float(statistics.median(s[0] for s in loaded)),
+            "sm_max_mhz": self.max_mhz,
+            "reasons": sorted(reasons),
+            "samples": len(self.samples),
+        }
+
+
+def ncu_traffic_per_launch(n: int):
+    """DRAM bytes per FP32 matvec launch from the committed ncu summary, if any."""
+    path = REPO / "profiles" / "k1_matvec_f32_n100000.md"
+    if not path.exists():
+        return None
+    m = re.search(r"traffic_bytes_per_launch_n%d:\s*([0-9.eE+]+)" % n, path.read_text())
+    return float(m.group(1)) if m else None
+
+
+def build_problem(n: int, seed: int, dev: torch.device):
+    import laker_b200 as L
+
+    x, y, _ = L.synthetic_field(n, seed)
+    emb = L.PositionEmbedding(2, EMBED_DIM, device=dev, dtype=torch.float32)
+    with torch.no_grad():
+        E = emb(x.to(dev))
+    op = L.AttentionKernelOperator(E, lambda_reg=LAMBDA)
+    pre = L.CCCPPreconditioner(num_probes=NUM_PROBES, gamma=0.1, verbose=False, device=dev,
+                               dtype=torch.float32).build(op.matvec, n, seed=0)
+    return op, pre, y.double()
+
+
+# ---------------------------------------------------------------------------
+# CPU reference (float64 oracle of the reference path) -- bounded sample
+# ---------------------------------------------------------------------------
+def reference_iterations(n: int) -> tuple[int, str]:
+    v = REFERENCE_ITERATIONS.get(n)
+    if v:
+        return int(v), "float64 reference recurrence iteration count measured on this system"
+    return REFERENCE_ITERATIONS_FALLBACK, "assumed float64 iteration count (not yet measured)"
+
+
+def cpu_reference_sample(n: int, seed: int, target_s: float) -> dict:
+    """Time one float64 PCG iteration of the reference path on the host.
+
+    Bounded: the n^2 matvec is timed on the first m rows (m sized so the sample
+    takes ~target_s) and scaled by n/m; the CCCP apply (n x 256 factors) and
+    the vector updates are timed in full.  solves/s = 1 / (t_iter * iters).
+    """
+    if not (REPO / "oracle" / "liblaker_oracle.so").exists():
+        subprocess.run(["make", "-s", "-C", str(REPO / "oracle")], check=True)
+    from oracle import laker_oracle as O
+    import laker_b200 as L
+
+    x, y, _ = L.synthetic_field(n, seed)
+    emb = L.PositionEmbedding(2, EMBED_DIM, device=torch.device("cpu"), dtype=torch.float32)
+    with torch.no_grad():
+        E = emb(x).double().numpy()
+    rng = np.random.default_rng(0)
+    v = rng.standard_normal(n)
+    m = 256
+    t = 0.0
+    while True:
+        t0 = time.perf_counter()
+        O.rect_matvec(E[:m], E, v)
+        t = time.perf_counter() - t0
+        if t >= 0.5 or m >= n:
+            break
+        m = min(n, m * 4)
+    m = int(min(n, max(m, m * target_s / max(t, 1e-6))))
+    t0 = time.perf_counter()
+    O.rect_matvec(E[:m], E, v)
+    t_rows = time.perf_counter() - t0
+    t_matvec = t_rows * n / m
+    q = rng.standard_normal((n, NUM_PROBES)) / math.sqrt(n)
+    state = {"isotropic_coef": 0.01, "q_basis": q, "q_eigenvalues": np.linspace(0.01, 1, NUM_PROBES),
+             "q_eigenvectors": np.eye(NUM_PROBES)}
+    t0 = time.perf_counter()
+    z = O.cccp_apply(state, v)
+    xx = v + 0.5 * z
+    rr = v - 0.5 * z
+    _ = float(rr @ z), float(np.linalg.norm(rr)), xx
+    t_rest = time.perf_counter() - t0
+    iters, how = reference_iterations(n)
+    t_iter = t_matvec + t_rest
+    return {
+        "solves_per_s": 1.0 / (t_iter * iters),
+        "t_iter_s": t_iter,
+        "iters": iters,
+        "cores": O.c_threads(),
+        "sample": (f"float64 oracle: {m} of {n} rows of one fused matvec ({t_rows:.1f} s, scaled "
+                   f"x{n / m:.1f}) + one N_r={NUM_PROBES} CCCP apply and vector updates = one PCG "
+                   f"iteration ({t_iter:.2f} s), x {iters} iterations ({how})"),
+    }
+
+
+def run_reference(args) -> None:
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return
+    n = args.n
+    for _ in range(args.warmup):
+        cpu_reference_sample(n, 0, args.ref_sample_s)
+    vals = []
+    last = None
+    t_begin = time.perf_counter()
+    for _ in range(args.steps):
+        last = cpu_reference_sample(n, 0, args.ref_sample_s)
+        vals.append(last["solves_per_s"])
+    wall = time.perf_counter() - t_begin
+    value = float(statistics.median(vals))
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": "solves/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 / value,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {
+            "workload": f"exact-kernel PCG solve n={n} d={EMBED_DIM} N_r={NUM_PROBES} tol={TOL} "
+                        "(true float64 residual), synthetic path-loss field seed 0",
+            "n": n,
+            "precision": "float64 (the reference's float32 default does not reach a 1e-6 true "
+                         "residual: 1e-2 at n=20k)",
+            "sample_wall_s": wall,
+        },
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": last["cores"],
+                         "kind": "port", "sample": last["sample"]},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args) -> None:
+    import torch.distributed as dist
+
+    import laker_b200 as L
+    from laker_b200 import _lib
+
+    rank, world, local = dist_info()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=dev)
+    n = args.n
+    op, pre, y = build_problem(n, seed=rank, dev=dev)
+    y_dev = y.to(dev)
+    peaks = _lib.measure_peaks(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+    pcg = L.PreconditionedConjugateGradient(tol=TOL, max_iter=MAX_ITER, verbose=False,
+                                            profile=True)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        pcg.solve(op.matvec, pre.apply, y_dev)
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(dev)
+    step_ms, iters, accurate, launches = [], [], [], 0
+    k1_ms, k1_count, k4_ms = 0.0, 0, 0.0
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for i in range(args.steps):
+        flush.zero_()
+        ev[i][0].record()
+        alpha = pcg.solve(op.matvec, pre.apply, y_dev)
+        ev[i][1].record()
+        res = pcg.last_result
+        iters.append(res.iterations)
+        accurate.append(res.accurate_matvecs)
+        launches += res.kernel_launches
+        k1_ms += res.fp32_matvec_ms
+        k1_count += res.fp32_matvec_launches
+        k4_ms += res.fp64_matvec_ms
+    torch.cuda.synchronize()
+    barrier()
+    clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(step_ms)
+    relres = pcg.residual_norm / float(torch.linalg.norm(y_dev))
+
+    # ---- end to end through the public API: pinned host y -> solve -> host alpha
+    y_host = y.clone().pin_memory()
+    e2e_ms = []
+    for i in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        yd = y_host.to(dev, non_blocking=True)
+        a = pcg.solve(op.matvec, pre.apply, yd)
+        a_host = a.to("cpu")
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_total = sum(e2e_ms)
+
+    if world > 1:
+        t = torch.tensor([total_ms, e2e_total], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, e2e_total = float(t[0]), float(t[1])
+        ent = torch.tensor([float(sum(iters) + sum(accurate))], device=dev, dtype=torch.float64)
+        dist.all_reduce(ent, op=dist.ReduceOp.SUM)
+        matvecs_all = float(ent[0])
+        lt = torch.tensor([launches], device=dev, dtype=torch.int64)
+        dist.all_reduce(lt, op=dist.ReduceOp.SUM)
+        launches_all = int(lt[0])
+    else:
+        matvecs_all = float(sum(iters) + sum(accurate))
+        launches_all = launches
+
+    if rank == 0:
+        solves = world * args.steps
+        value = solves / (total_ms / 1e3)
+        k1_avg_ms = k1_ms / max(k1_count, 1)
+        flops_per_launch = 2.0 * (EMBED_DIM + 1) * n * n  # d FMA logit + 1 FMA accumulate
+        achieved = flops_per_launch / (k1_avg_ms * 1e-3) / 1e12
+        traffic = ncu_traffic_per_launch(n)
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "solves/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": {
+                "workload": f"exact-kernel PCG solve n={n} d={EMBED_DIM} N_r={NUM_PROBES} "
+                            f"tol={TOL} (true float64 residual), synthetic path-loss field "
+                            f"seed=rank",
+                "n": n,
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                "precision": "FP32 fused operator in the recurrence; FP64 vectors, inner "
+                             "products, scalars and residual recomputation",
+                "l2": "flushed between steps (256 MB write)",
+            },
+            "kernel_entries_per_s": matvecs_all * n * n / (total_ms / 1e3),
+            "p50_ms": float(np.percentile(step_ms, 50)),
+            "p99_ms": float(np.percentile(step_ms, 99)),
+            "iterations": iters,
+            "fp64_residual_recomputations": accurate,
+            "relres_true": relres,
+            "e2e": {
+                "value": solves / (e2e_total / 1e3),
+                "unit": "solves/s",
+                "h2d_bytes_per_step": int(y_host.numel() * y_host.element_size()),
+                "d2h_bytes_per_step": int(a_host.numel() * a_host.element_size()),
+            },
+            "roofline": {
+                "bound": "fma",
+                "kernel": "k1_matvec_f32 (FP32 fused matvec)",
+                "achieved": achieved,
+                "peak": peaks["ffma_tflops"],
+                "unit": "TFLOP/s",
+                "frac": achieved / peaks["ffma_tflops"],
+                "traffic": traffic,
+                "avg_launch_ms": k1_avg_ms,
+                "algorithmic_flops_per_launch": flops_per_launch,
+                "peak_source": "FFMA microbenchmark measured in this run (laker_measure_peaks); "
+                               "nominal 148 SM x 128 FMA/clk x 2 flop x clock for context",
+                "nominal_peak_at_max_clock": 148 * 128 * 2 * 1.965e9 / 1e12,
+                "mufu_frac": (n * n / (k1_avg_ms * 1e-3)) / (peaks["mufu_tops"] * 1e12),
+                "fp64_matvec_ms_total": k4_ms,
+            },
+            "clocks": clocks.summary(),
+            "gpu_launches": launches_all,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            cb = cpu_reference_sample(n, 0, args.cpu_sample_s)
+            line["cpu_baseline"] = {"value": cb["solves_per_s"], "unit": "solves/s",
+                                    "cores": cb["cores"], "kind": "port", "sample": cb["sample"]}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def kernel_only(args) -> None:
+    """FP32 fused matvec alone on the bench embeddings (a clean ncu target)."""
+    import laker_b200 as L
+
+    dev = torch.device("cuda", 0)
+    x, _, _ = L.synthetic_field(args.n, 0)
+    emb = L.PositionEmbedding(2, EMBED_DIM, device=dev, dtype=torch.float32)
+    with torch.no_grad():
+        E = emb(x.to(dev))
+    op = L.AttentionKernelOperator(E, lambda_reg=LAMBDA)
+    v = torch.randn(args.n, device=dev)
+    for _ in range(args.warmup):
+        op.matvec(v)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        op.matvec(v)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    print(json.dumps({"kernel": "fp32 fused matvec", "n": args.n, "ms": ms,
+                      "entries_per_s": args.n * args.n / (ms * 1e-3)}))
+
+
+def count_reference_iterations(args) -> None:
+    """Iterations of the float64 reference recurrence on the bench system."""
+    import laker_b200  # noqa: F401
+    from oracle import laker_oracle as O
+
+    dev = torch.device("cuda", 0)
+    op, pre, y = build_problem(args.n, 0, dev)
+    state = {"isotropic_coef": pre.isotropic_coef, "q_basis": pre.q_basis.double().cpu().numpy(),
+             "q_eigenvalues": pre.q_eigenvalues.double().cpu().numpy(),
+             "q_eigenvectors": pre.q_eigenvectors.double().cpu().numpy()}
+
+    def apply_a(v):
+        return op.matvec_f64(torch.as_tensor(v, device=dev)).cpu().numpy()
+
+    x, iters, rn = O.pcg_solve(apply_a, lambda v: O.cccp_apply(state, v), y.numpy(), tol=TOL,
+                               max_iter=MAX_ITER)
+    true_rel = float(np.linalg.norm(y.numpy() - apply_a(x)) / np.linalg.norm(y.numpy()))
+    print(json.dumps({"n": args.n, "reference_iterations": iters, "recurrence_relres":
+                      rn / float(np.linalg.norm(y.numpy())), "true_relres": true_rel}))
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawTextHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-s", type=float, default=12.0)
+    ap.add_argument("--ref-sample-s", type=float, default=5.0)
+    ap.add_argument("--count-reference-iterations", action="store_true")
+    ap.add_argument("--kernel-only", action="store_true",
+                    help="time the FP32 fused matvec alone (profiling target)")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours" and not args.kernel_only:
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.kernel_only:
+        kernel_only(args)
+    elif args.count_reference_iterations:
+        count_reference_iterations(args)
+    elif args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

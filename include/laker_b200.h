@@ -164,6 +164,7 @@ typedef struct laker_pcg_params {
   double breakdown_eps;  /* breakdown test p^T A p <= -eps ||p|| ||Ap||     */
   int check_every;       /* host polls the device status every N iterations */
   int has_x0;            /* 1: X holds the initial guess on entry           */
+  int profile;           /* 1: time the fused matvec launches with events   */
 } laker_pcg_params;
 
 typedef struct laker_pcg_result {
@@ -173,6 +174,11 @@ typedef struct laker_pcg_result {
   double residual_norm;    /* ||b - A x||_F of the returned x (FP64 A)      */
   double rhs_norm;         /* ||b||_F                                       */
   double recurrence_norm;  /* last recurrence residual norm                 */
+  int kernel_launches;     /* kernels this call launched (all of them)      */
+  double fp32_matvec_ms;   /* profile: summed device time of FP32 matvecs   */
+  double fp64_matvec_ms;   /* profile: summed device time of FP64 matvecs   */
+  int fp32_matvec_launches;
+  int fp64_matvec_launches;
 } laker_pcg_result;
 
 size_t laker_pcg_workspace_bytes(int64_t n, int d, int nr, int k);

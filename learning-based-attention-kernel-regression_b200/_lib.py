@@ -71,6 +71,7 @@ class laker_pcg_params(ctypes.Structure):
         ("breakdown_eps", c_double),
         ("check_every", c_int),
         ("has_x0", c_int),
+        ("profile", c_int),
     ]
 
 
@@ -82,6 +83,11 @@ class laker_pcg_result(ctypes.Structure):
         ("residual_norm", c_double),
         ("rhs_norm", c_double),
         ("recurrence_norm", c_double),
+        ("kernel_launches", c_int),
+        ("fp32_matvec_ms", c_double),
+        ("fp64_matvec_ms", c_double),
+        ("fp32_matvec_launches", c_int),
+        ("fp64_matvec_launches", c_int),
     ]
 
 

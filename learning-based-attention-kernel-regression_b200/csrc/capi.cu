@@ -53,18 +53,38 @@ namespace {
 // Register-resident dependent chains, 16 independent chains per thread.
 constexpr int kPeakThreads = 256;
 
+// 32 independent packed-pair chains, 4x unrolled: 128 FFMA2 per loop trip.
 __global__ void __launch_bounds__(kPeakThreads) peak_ffma2_kernel(int iters, float seed, float* sink) {
-  float2 a[16];
+  float2 a[32];
 #pragma unroll
-  for (int q = 0; q < 16; ++q) a[q] = make_float2(seed + q, seed - q);
+  for (int q = 0; q < 32; ++q) a[q] = make_float2(seed + q, seed - q);
   const float2 m = make_float2(0.9999f, 0.9998f), c = make_float2(1e-6f, 2e-6f);
-  for (int it = 0; it < iters; ++it) {
+  for (int it = 0; it < iters; it += 4) {
 #pragma unroll
-    for (int q = 0; q < 16; ++q) a[q] = __ffma2_rn(a[q], m, c);
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int q = 0; q < 32; ++q) a[q] = __ffma2_rn(a[q], m, c);
   }
   float s = 0.0f;
 #pragma unroll
-  for (int q = 0; q < 16; ++q) s += a[q].x + a[q].y;
+  for (int q = 0; q < 32; ++q) s += a[q].x + a[q].y;
+  if (s == 1234.5678f) sink[0] = s;
+}
+
+// Same with scalar FFMA: 32 chains x 4 unroll.
+__global__ void __launch_bounds__(kPeakThreads) peak_ffma_kernel(int iters, float seed, float* sink) {
+  float a[32];
+#pragma unroll
+  for (int q = 0; q < 32; ++q) a[q] = seed + q;
+  for (int it = 0; it < iters; it += 4) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int q = 0; q < 32; ++q) a[q] = fmaf(a[q], 0.9999f, 1e-6f);
+  }
+  float s = 0.0f;
+#pragma unroll
+  for (int q = 0; q < 32; ++q) s += a[q];
   if (s == 1234.5678f) sink[0] = s;
 }
 
@@ -155,10 +175,15 @@ extern "C" int laker_measure_peaks(void* scratch, double* ffma_tflops, double* m
   float ms = 0.0f;
   int st;
   if (ffma_tflops) {
-    const int iters = 8192;
+    // best of packed (FFMA2) and scalar FFMA chains; 2 flops per FMA
+    const int iters = 4096;
     st = time_kernel([&] { peak_ffma2_kernel<<<grid, kPeakThreads, 0, s>>>(iters, 1.0f, f); }, s, &ms);
     if (st) return st;
-    *ffma_tflops = threads * iters * 16.0 * 2.0 * 2.0 / (ms * 1e-3) / 1e12;  // 2 FMA x 2 flop
+    const double packed = threads * iters * 32.0 * 2.0 * 2.0 / (ms * 1e-3) / 1e12;
+    st = time_kernel([&] { peak_ffma_kernel<<<grid, kPeakThreads, 0, s>>>(iters, 1.0f, f); }, s, &ms);
+    if (st) return st;
+    const double scalar = threads * iters * 32.0 * 2.0 / (ms * 1e-3) / 1e12;
+    *ffma_tflops = packed > scalar ? packed : scalar;
   }
   if (mufu_tops) {
     const int iters = 2048;

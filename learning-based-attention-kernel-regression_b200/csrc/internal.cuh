@@ -25,6 +25,7 @@ int sm_count();
 struct SegPlan {
   int S;
   int64_t cols_per_seg;
+  int cfg = 0;  // kernel variant (rows per thread / threads per CTA)
 };
 SegPlan plan_segments(int64_t m, int64_t n, int rows_per_cta, int ctas_per_sm, int tile);
 

@@ -11,6 +11,8 @@
 // CTA reduces its segment into FP64 row partials; nothing of size n^2 is ever
 // stored.  Algorithmic work per entry: d FMA (logit) + 1 FMA (accumulate) +
 // 1 exp2.
+#include <cstdlib>
+
 #include "internal.cuh"
 
 namespace laker {
@@ -141,14 +143,85 @@ __global__ void __launch_bounds__(T, 2)
   }
 }
 
+// K1 variants: rows per thread x threads per CTA.  Variant 0 is compiled for
+// every padded dimension; the others only for d = 9..10 (the LAKER default),
+// where the tile-shape autotuner picks among them.
+struct K1Variant {
+  int rows, threads;
+};
+constexpr K1Variant kK1Variants[] = {{2, 256}, {4, 256}, {2, 128}, {4, 128}, {3, 256}};
+constexpr int kK1NumVariants = sizeof(kK1Variants) / sizeof(kK1Variants[0]);
+
+template <int DP, int R, int TT, bool CLAMP>
+cudaError_t launch_k1_rt(const float* rows, int64_t m, const float* cols, int64_t n,
+                         const float* x, double* part, const SegPlan& p, int* status,
+                         const int* gate, cudaStream_t s) {
+  dim3 grid((unsigned)ceil_div(m, TT * R), (unsigned)p.S);
+  k1_matvec_f32<DP, R, TT, CLAMP>
+      <<<grid, TT, 0, s>>>(rows, m, cols, n, x, part, p.cols_per_seg, status, gate);
+  return cudaGetLastError();
+}
+
 template <int DP, bool CLAMP>
 cudaError_t launch_k1_t(const float* rows, int64_t m, const float* cols, int64_t n,
                         const float* x, double* part, const SegPlan& p, int* status,
                         const int* gate, cudaStream_t s) {
-  dim3 grid((unsigned)ceil_div(m, kK1Threads * kK1Rows), (unsigned)p.S);
-  k1_matvec_f32<DP, kK1Rows, kK1Threads, CLAMP>
-      <<<grid, kK1Threads, 0, s>>>(rows, m, cols, n, x, part, p.cols_per_seg, status, gate);
-  return cudaGetLastError();
+  if constexpr (DP == 10) {
+    switch (p.cfg) {
+      case 1: return launch_k1_rt<DP, 4, 256, CLAMP>(rows, m, cols, n, x, part, p, status, gate, s);
+      case 2: return launch_k1_rt<DP, 2, 128, CLAMP>(rows, m, cols, n, x, part, p, status, gate, s);
+      case 3: return launch_k1_rt<DP, 4, 128, CLAMP>(rows, m, cols, n, x, part, p, status, gate, s);
+      case 4: return launch_k1_rt<DP, 3, 256, CLAMP>(rows, m, cols, n, x, part, p, status, gate, s);
+      default: break;
+    }
+  }
+  return launch_k1_rt<DP, kK1Rows, kK1Threads, CLAMP>(rows, m, cols, n, x, part, p, status, gate, s);
+}
+
+// Resident CTAs per SM of a K1 variant (occupancy API; 2 when unavailable).
+int k1_occupancy(int cfg, int dp) {
+  static int cache[kK1NumVariants][9] = {};
+  if (cfg < 0 || cfg >= kK1NumVariants || dp < 2 || dp > 16) return 2;
+  int& c = cache[cfg][dp / 2];
+  if (c > 0) return c;
+  int nb = 0;
+  cudaError_t e = cudaErrorInvalidValue;
+  const void* fn = nullptr;
+#define LAKER_K1_FN(DPv)                                                               \
+  if (dp == DPv) fn = reinterpret_cast<const void*>(&k1_matvec_f32<DPv, kK1Rows, kK1Threads, false>);
+  LAKER_K1_FN(2) LAKER_K1_FN(4) LAKER_K1_FN(6) LAKER_K1_FN(8) LAKER_K1_FN(12) LAKER_K1_FN(14)
+  LAKER_K1_FN(16)
+#undef LAKER_K1_FN
+  if (dp == 10) {
+    switch (cfg) {
+      case 1: fn = reinterpret_cast<const void*>(&k1_matvec_f32<10, 4, 256, false>); break;
+      case 2: fn = reinterpret_cast<const void*>(&k1_matvec_f32<10, 2, 128, false>); break;
+      case 3: fn = reinterpret_cast<const void*>(&k1_matvec_f32<10, 4, 128, false>); break;
+      case 4: fn = reinterpret_cast<const void*>(&k1_matvec_f32<10, 3, 256, false>); break;
+      default: fn = reinterpret_cast<const void*>(&k1_matvec_f32<10, kK1Rows, kK1Threads, false>);
+    }
+  }
+  const int threads = (dp == 10) ? kK1Variants[cfg].threads : kK1Threads;
+  if (fn) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, 0);
+  if (e != cudaSuccess || nb < 1) {
+    cudaGetLastError();
+    nb = 2;
+  }
+  c = nb;
+  return c;
+}
+
+// Variant choice: LAKER_K1_VARIANT overrides (tuning sweeps); otherwise the
+// default variant.
+int k1_variant(int dp) {
+  if (dp != 10) return 0;
+  static int v = -1;
+  if (v < 0) {
+    const char* s = getenv("LAKER_K1_VARIANT");
+    v = s ? atoi(s) : 0;
+    if (v < 0 || v >= kK1NumVariants) v = 0;
+  }
+  return v;
 }
 
 // ---------------------------------------------------------------------------
@@ -322,8 +395,12 @@ __global__ void finish_f32_kernel(const double* __restrict__ part, int S, int64_
 }  // namespace
 
 SegPlan k1_plan(int64_t m, int64_t n, int d) {
-  (void)d;
-  return plan_segments(m, n, kK1Threads * kK1Rows, 2, kTileCols32);
+  const int dp = padded_dim(d);
+  const int cfg = k1_variant(dp);
+  const K1Variant v = kK1Variants[cfg];
+  SegPlan p = plan_segments(m, n, v.rows * v.threads, k1_occupancy(cfg, dp), kTileCols32);
+  p.cfg = cfg;
+  return p;
 }
 
 cudaError_t launch_k1(const float* rows32, int64_t m, const float* cols32, int64_t n, int d,

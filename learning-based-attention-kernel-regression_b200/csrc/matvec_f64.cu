@@ -152,9 +152,30 @@ __global__ void finish_f64_kernel(const double* __restrict__ part, int S, int64_
 
 }  // namespace
 
+// Resident CTAs per SM of the FP64 kernel (occupancy API; 2 when unavailable).
+int k4_occupancy(int dp) {
+  static int cache[9] = {};
+  if (dp < 2 || dp > 16) return 2;
+  int& c = cache[dp / 2];
+  if (c > 0) return c;
+  const void* fn = nullptr;
+#define LAKER_K4_FN(DPv) \
+  if (dp == DPv) fn = reinterpret_cast<const void*>(&k4_matvec_f64<DPv, kK4Rows, kK4Threads, false>);
+  LAKER_K4_FN(2) LAKER_K4_FN(4) LAKER_K4_FN(6) LAKER_K4_FN(8) LAKER_K4_FN(10) LAKER_K4_FN(12)
+  LAKER_K4_FN(14) LAKER_K4_FN(16)
+#undef LAKER_K4_FN
+  int nb = 0;
+  if (!fn || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kK4Threads, 0) != cudaSuccess ||
+      nb < 1) {
+    cudaGetLastError();
+    nb = 2;
+  }
+  c = nb;
+  return c;
+}
+
 SegPlan k4_plan(int64_t m, int64_t n, int d) {
-  (void)d;
-  return plan_segments(m, n, kK4Threads * kK4Rows, 2, kTileCols64);
+  return plan_segments(m, n, kK4Threads * kK4Rows, k4_occupancy(padded_dim(d)), kTileCols64);
 }
 
 cudaError_t launch_k4(const double* rows64, int64_t m, const double* cols64, int64_t n, int d,

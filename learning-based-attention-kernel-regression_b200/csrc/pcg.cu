@@ -231,6 +231,40 @@ __global__ void __launch_bounds__(T)
   }
 }
 
+// Optional per-launch CUDA-event timing of the fused matvecs (params.profile):
+// events bracket each launch on the solve's stream and are read after the
+// status poll that synchronises it.
+struct LaunchTimer {
+  static constexpr int kMax = 64;
+  bool on = false;
+  int used = 0, count = 0;
+  double total_ms = 0.0;
+  cudaEvent_t ev[2 * kMax];
+  void init(bool enable) {
+    on = enable;
+    if (!on) return;
+    for (auto& e : ev)
+      if (cudaEventCreate(&e) != cudaSuccess) on = false;
+  }
+  void begin(cudaStream_t s) {
+    if (on && used < kMax) cudaEventRecord(ev[2 * used], s);
+  }
+  void end(cudaStream_t s) {
+    if (on && used < kMax) cudaEventRecord(ev[2 * used + 1], s), ++used;
+  }
+  void collect() {
+    for (int i = 0; i < used; ++i) {
+      float ms = 0.0f;
+      if (cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]) == cudaSuccess) total_ms += ms, ++count;
+    }
+    used = 0;
+  }
+  ~LaunchTimer() {
+    if (on)
+      for (auto& e : ev) cudaEventDestroy(e);
+  }
+};
+
 // Workspace carve-up of one single-RHS solve.
 struct PcgWs {
   WsHeader* hdr;
@@ -317,6 +351,10 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
   if (e != cudaSuccess) return fail_cuda(e);
 
   int* dstatus = &w.hdr->status;
+  int launches = 0;
+  LaunchTimer t32, t64;
+  t32.init(prm->profile != 0);
+  t64.init(prm->profile != 0);
   auto launch_precond = [&](int init) {
     if (pc) {
       pc_project_kernel<T><<<Gp, T, 0, s>>>(view, w.r, w.upart, w.v, &w.st->counters[kCtrProject],
@@ -324,14 +362,18 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
       pc_expand_kernel<T, float><<<Gp, T, 0, s>>>(view, w.r, w.v, w.z, w.blockpart,
                                                  &w.st->counters[kCtrExpand], w.st, init, nullptr,
                                                  &w.st->active);
+      launches += 2;
     } else {
       identity_expand_kernel<<<G, T, 0, s>>>(w.r, w.z, n, w.blockpart, w.st, init);
+      launches += 1;
     }
     pcg_update_p_kernel<<<G, T, 0, s>>>(w.z, w.p, n, w.st, init);
+    launches += 1;
   };
 
   // ---- initialisation ------------------------------------------------------
   pcg_init_kernel<<<G, T, 0, s>>>(B, X, w.r, n, prm->has_x0, prm->tol, w.blockpart, w.st);
+  launches += 1;
   e = cudaGetLastError();
   if (e != cudaSuccess) return fail_cuda(e);
   if (prm->has_x0) {
@@ -339,11 +381,13 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
     e = launch_k4(op->packed64, n, op->packed64, n, d, op->clamp, X, w.part64, p4, dstatus, nullptr, s);
     if (e != cudaSuccess) return fail_cuda(e);
     pcg_after_residual_kernel<<<G, T, 0, s>>>(w.part64, p4.S, B, X, w.r, n, 1, w.blockpart, w.st);
+    launches += 2;
   }
   e = cudaMemcpyAsync(&h, w.st, sizeof(PcgState), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return fail_cuda(e);
   res->rhs_norm = h.bnorm;
+  res->kernel_launches = launches;
   if (h.bnorm == 0.0) {
     // zero right-hand side: x is returned unchanged (zero, or x0), as in
     // laker/solvers.py:177-182
@@ -365,19 +409,24 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
     const double est_s = (double)n * (double)n / 2e12 + 40e-6;
     check = (int)(0.01 / est_s);
     if (check < 1) check = 1;
-    if (check > 64) check = 64;
   }
+  if (check > LaunchTimer::kMax) check = LaunchTimer::kMax;
   int launched = 0;
   while (launched < prm->max_iter) {
     const int chunk = (prm->max_iter - launched) < check ? (prm->max_iter - launched) : check;
     for (int c = 0; c < chunk; ++c) {
+      t32.begin(s);
       launch_k1(op->packed32, n, op->packed32, n, d, op->clamp, w.p, w.part32, p1, dstatus,
                 &w.st->active, s);
+      t32.end(s);
       pcg_after_matvec_kernel<<<G, T, 0, s>>>(w.part32, p1.S, w.p, w.Ap, n, w.blockpart, w.st);
       pcg_update_xr_kernel<<<G, T, 0, s>>>(w.p, w.Ap, X, w.r, n, w.blockpart, w.st);
+      t64.begin(s);
       launch_k4(op->packed64, n, op->packed64, n, d, op->clamp, X, w.part64, p4, dstatus,
                 &w.st->need_update, s);
+      t64.end(s);
       pcg_after_residual_kernel<<<G, T, 0, s>>>(w.part64, p4.S, B, X, w.r, n, 0, w.blockpart, w.st);
+      launches += 5;
       launch_precond(0);
     }
     launched += chunk;
@@ -385,6 +434,8 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
     if (e == cudaSuccess) e = cudaMemcpyAsync(&h, w.st, sizeof(PcgState), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return fail_cuda(e);
+    t32.collect();
+    t64.collect();
     if (h.done) break;
   }
 
@@ -396,6 +447,11 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
   res->residual_norm = h.true_rnorm;
   res->recurrence_norm = h.rnorm;
   res->rhs_norm = h.bnorm;
+  res->kernel_launches = launches;
+  res->fp32_matvec_ms = t32.total_ms;
+  res->fp32_matvec_launches = t32.count;
+  res->fp64_matvec_ms = t64.total_ms;
+  res->fp64_matvec_launches = t64.count;
   if (dev_status != 0) {
     res->status = dev_status;
     return dev_status;

@@ -68,6 +68,7 @@ class PreconditionedConjugateGradient:
         autograd_safe: bool = False,
         reliable_delta: float = 0.1,
         check_every: int = 0,
+        profile: bool = False,
     ) -> None:
         self.tol = float(tol)
         self.max_iter = max_iter
@@ -77,6 +78,8 @@ class PreconditionedConjugateGradient:
         self.autograd_safe = autograd_safe
         self.reliable_delta = float(reliable_delta)
         self.check_every = int(check_every)
+        self.profile = bool(profile)
+        self.last_result: Optional[_lib.laker_pcg_result] = None
         self.iterations: int = 0
         self.residual_norm: float = float("inf")
         self.accurate_matvecs: int = 0
@@ -136,10 +139,11 @@ class PreconditionedConjugateGradient:
             x = torch.empty_like(b)
         params = _lib.laker_pcg_params(
             self.tol, int(max_iter), self.reliable_delta, self._eps(rhs.dtype), self.check_every,
-            int(x0 is not None),
+            int(x0 is not None), int(self.profile),
         )
         res = _lib.pcg_solve(op.c_operator(), pc.c_precond() if pc is not None else None, b, x,
                              params)
+        self.last_result = res
         self.iterations = int(res.iterations)
         self.accurate_matvecs = int(res.accurate_matvecs)
         self.residual_norm = float(res.residual_norm)
