@@ -128,11 +128,13 @@ int laker_kernel_eval(const double* rows64, int64_t m, const double* cols64, int
 /* Factored CCCP preconditioner                                              */
 /* ------------------------------------------------------------------------ */
 typedef struct laker_precond {
-  const float* q_basis; /* (n x nr) row-major, orthonormal columns Q          */
+  const float* q_basis; /* (n x ldq) row-major, orthonormal columns Q in the
+                           first nr columns, zeros after; 16-byte aligned     */
   const float* w_core;  /* (nr x nr) row-major W = V diag(l^-1/2 - c^-1/2) V^T */
   int64_t n;
-  int nr;
-  double inv_sqrt_iso; /* c^-1/2, c = isotropic coefficient                  */
+  int nr;               /* 1 <= nr <= 1024                                   */
+  int ldq;              /* leading dimension of q_basis: multiple of 4, >= nr */
+  double inv_sqrt_iso;  /* c^-1/2, c = isotropic coefficient                 */
 } laker_precond;
 
 size_t laker_precond_workspace_bytes(int64_t n, int nr, int k);

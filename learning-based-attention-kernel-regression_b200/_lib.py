@@ -48,6 +48,7 @@ class laker_precond(ctypes.Structure):
         ("w_core", c_void_p),
         ("n", c_int64),
         ("nr", c_int),
+        ("ldq", c_int),
         ("inv_sqrt_iso", c_double),
     ]
 
@@ -289,8 +290,18 @@ def kernel_eval(rows64, m, cols64, p, d, clamp, out_dtype, device) -> torch.Tens
     return out
 
 
+def padded_q(q: torch.Tensor) -> torch.Tensor:
+    """FP32 copy of Q (n x nr) with rows padded to a multiple of 4 columns (zeros)."""
+    n, nr = q.shape
+    ldq = (nr + 3) // 4 * 4
+    out = torch.zeros((n, ldq), dtype=torch.float32, device=q.device)
+    out[:, :nr] = q
+    return out
+
+
 def precond_struct(q32, w32, n, nr, cis) -> laker_precond:
-    return laker_precond(ptr(q32), ptr(w32), n, nr, float(cis))
+    """Descriptor of the fused apply's factors; q32 from padded_q()."""
+    return laker_precond(ptr(q32), ptr(w32), n, nr, int(q32.shape[1]), float(cis))
 
 
 def precond_apply(pc: laker_precond, R: torch.Tensor, out_dtype) -> torch.Tensor:

@@ -1,5 +1,5 @@
-// Device-resident state of one PCG solve and the single-RHS kernels that the
-// preconditioner apply and the PCG loop share.
+// Device-resident state of one PCG solve and the single-RHS preconditioner
+// kernels shared by the standalone apply and the PCG loop.
 #pragma once
 
 #include "internal.cuh"
@@ -15,7 +15,7 @@ struct alignas(256) PcgState {
   double pAp;         // p . A p
   double alpha, beta;
   double rnorm;       // recurrence residual norm (after the last update)
-  double rmax;        // residual norm at the last FP64 recomputation
+  double rmax;        // max recurrence residual norm since the last FP64 recomputation
   double true_rnorm;  // ||b - A x|| from the last FP64 recomputation
   double delta;       // reliable-update factor
   double eps;         // breakdown threshold
@@ -36,94 +36,146 @@ enum { kCtrBnorm = 0, kCtrMatvec, kCtrUpdate, kCtrResid, kCtrProject, kCtrExpand
 
 constexpr int kMaxNr = 1024;  // largest probe count of the fused apply
 constexpr int kVecThreads = 256;
+constexpr int kPcChunkCols = 128;  // columns covered by one float4 per lane of a warp
 
 struct PcView {
-  const float* Q;  // (n x nr) row-major
+  const float* Q;  // (n x ldq) row-major, columns nr..ldq-1 zero, rows 16-byte aligned
   const float* W;  // (nr x nr) symmetric
   int64_t n;
   int nr;
+  int ldq;     // multiple of 4
   double cis;  // c^-1/2
 };
 
-// u = Q^T r (per-block FP64 partials, fixed-order total in the last block),
-// then v = W u.  One pass over Q; thread t owns columns t, t+T, ...
-template <int T>
+// Rows a warp keeps in flight so that every lane has ~8 float4 loads pending.
+template <int NCH>
+struct PcRows {
+  static constexpr int value = NCH >= 8 ? 1 : 8 / NCH;
+};
+
+// u = Q^T r, then v = W u.  One pass over Q: each warp walks rows with float4
+// loads (lane l covers columns 4l + 128 j), keeping several rows in flight;
+// per-warp FP32 column sums are combined in FP64 per block, and the last block
+// forms the fixed-order FP64 total and v = W u.  HBM-bound: n * ldq * 4 bytes.
+template <int T, int NCH>
 __global__ void __launch_bounds__(T)
     pc_project_kernel(PcView pc, const double* __restrict__ r, double* __restrict__ upart,
                       double* __restrict__ v, unsigned int* counter, const int* gate) {
   if (gate && *gate == 0) return;
-  constexpr int NQ = kMaxNr / T;
-  __shared__ double s_r[T];
+  constexpr int RW = PcRows<NCH>::value;
+  constexpr int NW = T / 32;
+  __shared__ __align__(16) float s_w[NW][NCH * kPcChunkCols];
   __shared__ double s_u[kMaxNr];
-  const int tid = threadIdx.x;
-  const int nr = pc.nr;
-  const int64_t per = ceil_div(pc.n, (int64_t)gridDim.x);
-  const int64_t i_begin = (int64_t)blockIdx.x * per;
-  const int64_t i_end = min(pc.n, i_begin + per);
-  double acc[NQ];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int ldq4 = pc.ldq >> 2;
+  const float4* Q4 = reinterpret_cast<const float4*>(pc.Q);
+  float4 acc[NCH];
 #pragma unroll
-  for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
-  for (int64_t i0 = i_begin; i0 < i_end; i0 += T) {
-    const int cnt = (int)min((int64_t)T, i_end - i0);
-    __syncthreads();
-    if (tid < cnt) s_r[tid] = r[i0 + tid];
-    __syncthreads();
-    for (int ii = 0; ii < cnt; ++ii) {
-      const double ri = s_r[ii];
-      const float* qrow = pc.Q + (i0 + ii) * nr;
+  for (int ch = 0; ch < NCH; ++ch) acc[ch] = make_float4(0.f, 0.f, 0.f, 0.f);
+  const int64_t nwarps = (int64_t)gridDim.x * NW;
+  const int64_t wid = (int64_t)blockIdx.x * NW + warp;
+  for (int64_t i0 = wid; i0 < pc.n; i0 += nwarps * RW) {
+    float rv[RW];
+    float4 q[RW][NCH];
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) {
-        const int c = tid + q * T;
-        if (c < nr) acc[q] = fma((double)qrow[c], ri, acc[q]);
+    for (int u = 0; u < RW; ++u) {
+      const int64_t i = i0 + (int64_t)u * nwarps;
+      const bool ok = i < pc.n;
+      rv[u] = ok ? (float)r[i] : 0.0f;
+#pragma unroll
+      for (int ch = 0; ch < NCH; ++ch) {
+        const int c4 = lane + 32 * ch;
+        q[u][ch] = (ok && c4 < ldq4) ? __ldg(Q4 + i * ldq4 + c4) : make_float4(0.f, 0.f, 0.f, 0.f);
       }
     }
+#pragma unroll
+    for (int u = 0; u < RW; ++u)
+#pragma unroll
+      for (int ch = 0; ch < NCH; ++ch) {
+        acc[ch].x = fmaf(q[u][ch].x, rv[u], acc[ch].x);
+        acc[ch].y = fmaf(q[u][ch].y, rv[u], acc[ch].y);
+        acc[ch].z = fmaf(q[u][ch].z, rv[u], acc[ch].z);
+        acc[ch].w = fmaf(q[u][ch].w, rv[u], acc[ch].w);
+      }
   }
 #pragma unroll
-  for (int q = 0; q < NQ; ++q) {
-    const int c = tid + q * T;
-    if (c < nr) upart[(int64_t)blockIdx.x * nr + c] = acc[q];
+  for (int ch = 0; ch < NCH; ++ch)
+    reinterpret_cast<float4*>(s_w[warp])[lane + 32 * ch] = acc[ch];
+  __syncthreads();
+  for (int c = threadIdx.x; c < pc.ldq; c += T) {
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) s += (double)s_w[w][c];
+    upart[(int64_t)blockIdx.x * pc.ldq + c] = s;
   }
   if (!arrive_last_block(counter)) return;
-  for (int c = tid; c < nr; c += T) {
+  const int nr = pc.nr;
+  for (int c = threadIdx.x; c < nr; c += T) {
     double u = 0.0;
-    for (unsigned int b = 0; b < gridDim.x; ++b) u += __ldcg(upart + (int64_t)b * nr + c);
+    for (unsigned int b = 0; b < gridDim.x; ++b) u += __ldcg(upart + (int64_t)b * pc.ldq + c);
     s_u[c] = u;
   }
   __syncthreads();
-  for (int c = tid; c < nr; c += T) {
+  for (int c = threadIdx.x; c < nr; c += T) {
     double acc2 = 0.0;
     for (int cc = 0; cc < nr; ++cc) acc2 = fma((double)pc.W[(int64_t)cc * nr + c], s_u[cc], acc2);
     v[c] = acc2;
   }
 }
 
-// z = c^-1/2 r + Q v (one warp per row) and the fixed-order total of r . z.
-// With a PcgState the last block turns r . z into beta (or seeds rz when
-// `init`); without one it stores the total in dot_out (if non-null).
-template <int T, typename ZT>
+// z = c^-1/2 r + Q v (one warp per row, float4 loads, several rows in flight)
+// and the fixed-order total of r . z.  With a PcgState the last block turns
+// r . z into beta (or seeds rz when `init`); without one it stores the total
+// in dot_out (if non-null).  HBM-bound: n * ldq * 4 bytes.
+template <int T, int NCH, typename ZT>
 __global__ void __launch_bounds__(T)
     pc_expand_kernel(PcView pc, const double* __restrict__ r, const double* __restrict__ v,
                      ZT* __restrict__ z, double* __restrict__ blockpart, unsigned int* counter,
                      PcgState* st, int init, double* dot_out, const int* gate) {
   if (gate && *gate == 0) return;
-  __shared__ double s_v[kMaxNr];
-  __shared__ double s_red[T / 32];
+  constexpr int RW = PcRows<NCH>::value;
+  constexpr int NW = T / 32;
+  __shared__ __align__(16) float s_v[NCH * kPcChunkCols];
+  __shared__ double s_red[NW];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int nr = pc.nr;
-  for (int c = tid; c < nr; c += T) s_v[c] = v[c];
+  for (int c = tid; c < NCH * kPcChunkCols; c += T) s_v[c] = (c < pc.nr) ? (float)v[c] : 0.0f;
   __syncthreads();
+  const int ldq4 = pc.ldq >> 2;
+  const float4* Q4 = reinterpret_cast<const float4*>(pc.Q);
+  const float4* V4 = reinterpret_cast<const float4*>(s_v);
   double dot = 0.0;
-  const int64_t nwarps = (int64_t)gridDim.x * (T / 32);
-  for (int64_t i = (int64_t)blockIdx.x * (T / 32) + warp; i < pc.n; i += nwarps) {
-    const float* qrow = pc.Q + i * nr;
-    double s = 0.0;
-    for (int c = lane; c < nr; c += 32) s = fma((double)qrow[c], s_v[c], s);
-    s = warp_sum(s);
-    if (lane == 0) {
-      const double ri = r[i];
-      const ZT zi = (ZT)(pc.cis * ri + s);
-      z[i] = zi;
-      dot = fma(ri, (double)zi, dot);
+  const int64_t nwarps = (int64_t)gridDim.x * NW;
+  for (int64_t i0 = (int64_t)blockIdx.x * NW + warp; i0 < pc.n; i0 += nwarps * RW) {
+    float4 q[RW][NCH];
+#pragma unroll
+    for (int u = 0; u < RW; ++u) {
+      const int64_t i = i0 + (int64_t)u * nwarps;
+#pragma unroll
+      for (int ch = 0; ch < NCH; ++ch) {
+        const int c4 = lane + 32 * ch;
+        q[u][ch] = (i < pc.n && c4 < ldq4) ? __ldg(Q4 + i * ldq4 + c4)
+                                           : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < RW; ++u) {
+      const int64_t i = i0 + (int64_t)u * nwarps;
+      float s = 0.0f;
+#pragma unroll
+      for (int ch = 0; ch < NCH; ++ch) {
+        const float4 vv = V4[lane + 32 * ch];
+        s = fmaf(q[u][ch].x, vv.x, s);
+        s = fmaf(q[u][ch].y, vv.y, s);
+        s = fmaf(q[u][ch].z, vv.z, s);
+        s = fmaf(q[u][ch].w, vv.w, s);
+      }
+      s = warp_sum(s);
+      if (lane == 0 && i < pc.n) {
+        const double ri = r[i];
+        const ZT zi = (ZT)(pc.cis * ri + (double)s);
+        z[i] = zi;
+        dot = fma(ri, (double)zi, dot);
+      }
     }
   }
   double vals[1] = {dot};
@@ -154,6 +206,35 @@ __global__ void __launch_bounds__(T)
       }
     }
   }
+}
+
+// Number of 128-column chunks (float4 per lane) of a padded Q row.
+inline int pc_chunks(int ldq) { return (ldq + kPcChunkCols - 1) / kPcChunkCols; }
+
+#define LAKER_PC_DISPATCH(nch, ...)                          \
+  switch (nch) {                                              \
+    case 1: { constexpr int NC = 1; __VA_ARGS__; } break;     \
+    case 2: { constexpr int NC = 2; __VA_ARGS__; } break;     \
+    case 3: { constexpr int NC = 3; __VA_ARGS__; } break;     \
+    case 4: { constexpr int NC = 4; __VA_ARGS__; } break;     \
+    case 5: { constexpr int NC = 5; __VA_ARGS__; } break;     \
+    case 6: { constexpr int NC = 6; __VA_ARGS__; } break;     \
+    case 7: { constexpr int NC = 7; __VA_ARGS__; } break;     \
+    default: { constexpr int NC = 8; __VA_ARGS__; } break;    \
+  }
+
+// The two-pass apply, z = P r: projection then expansion on stream s.
+template <typename ZT>
+inline void launch_precond_apply(const PcView& pc, int grid, const double* r, double* upart,
+                                 double* v, ZT* z, double* blockpart, unsigned int* ctr_project,
+                                 unsigned int* ctr_expand, PcgState* st, int init,
+                                 double* dot_out, const int* gate, cudaStream_t s) {
+  LAKER_PC_DISPATCH(pc_chunks(pc.ldq), {
+    pc_project_kernel<kVecThreads, NC><<<grid, kVecThreads, 0, s>>>(pc, r, upart, v, ctr_project,
+                                                                    gate);
+    pc_expand_kernel<kVecThreads, NC, ZT><<<grid, kVecThreads, 0, s>>>(
+        pc, r, v, z, blockpart, ctr_expand, st, init, dot_out, gate);
+  });
 }
 
 }  // namespace laker

@@ -177,7 +177,7 @@ class CCCPPreconditioner:
         scale = self.q_eigenvalues.to(torch.float64).rsqrt() - self.isotropic_coef ** (-0.5)
         w = (v * scale.unsqueeze(0)) @ v.T
         w = 0.5 * (w + w.T)
-        self._q32 = self.q_basis.to(torch.float32).contiguous()
+        self._q32 = _lib.padded_q(self.q_basis)
         self._w32 = w.to(torch.float32).contiguous()
         self._c = _lib.precond_struct(self._q32, self._w32, self.n, self.nr,
                                       self.isotropic_coef ** (-0.5))
@@ -205,7 +205,7 @@ class CCCPPreconditioner:
     def apply_2d(self, x: torch.Tensor) -> torch.Tensor:
         _lib.require_cuda(x, "x")
         # k right-hand sides: three plain GEMMs (cuBLAS) with the same folded W
-        q = self._q32.to(x.dtype)
+        q = self._q32[:, : self.nr].to(x.dtype)
         w = self._w32.to(x.dtype)
         return (self.isotropic_coef ** (-0.5)) * x + q @ (w @ (q.T @ x))
 

@@ -66,7 +66,7 @@ class PreconditionedConjugateGradient:
         restart_freq: Optional[int] = None,
         breakdown_eps: Optional[float] = None,
         autograd_safe: bool = False,
-        reliable_delta: float = 0.1,
+        reliable_delta: float = 0.05,
         check_every: int = 0,
         profile: bool = False,
     ) -> None:
@@ -189,6 +189,7 @@ class PreconditionedConjugateGradient:
             r.sub_(ap * alpha.unsqueeze(0))
             rn = torch.linalg.norm(r).item()
             self.recurrence_norm = rn
+            rmax = max(rmax, rn)  # running max since the last FP64 recomputation
             if rn <= self.reliable_delta * rmax or rn <= self.tol * bn or it == max_iter:
                 r = op.residual_f64(x, b)
                 self.accurate_matvecs += 1

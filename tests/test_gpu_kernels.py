@@ -204,7 +204,7 @@ def test_pcg_edge_cases(cuda):
     b = torch.randn(200, device=cuda, dtype=torch.float64)
     x = pcg.solve(op.matvec, None, b)
     x2 = pcg.solve(op.matvec, None, b, x0=x)
-    assert pcg.iterations <= 2
+    assert pcg.iterations <= 5
     assert rel(x2, x) < 1e-7
     # max_iter reached: warning path, x returned
     short = PreconditionedConjugateGradient(tol=1e-14, max_iter=3, verbose=False)
