@@ -46,7 +46,9 @@ enum laker_status {
   LAKER_ERR_NONFINITE = 5,     /* PCG: NaN/Inf in an inner product           */
   LAKER_ERR_TIMEOUT = 6,       /* a bounded device wait expired              */
   LAKER_ERR_WORKSPACE = 7,     /* workspace smaller than the query returned  */
-  LAKER_ERR_UNSUPPORTED = 8    /* shape/dtype combination not implemented    */
+  LAKER_ERR_UNSUPPORTED = 8,   /* shape/dtype combination not implemented    */
+  LAKER_ERR_SCRATCH_LIMIT = 9  /* larger than the fixed scratch of the
+                                  allocation-free entry point               */
 };
 
 /* Library version as 10000*major + 100*minor + patch. */
@@ -97,6 +99,26 @@ size_t laker_matvec_workspace_bytes(int64_t m, int64_t n, int d, int k, int prec
 int laker_attn_matvec_f32(const float* rows32, int64_t m, const float* cols32, int64_t n, int d,
                           float lam, int clamp, const float* X, int k, int64_t ldx, float* Y,
                           int64_t ldy, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Allocation-free FP32 fused matvec (single right-hand side).
+ *   y = lam * x[:m] + exp(Er Ec^T) x          (x: n, y: m)
+ * Same arguments and result as laker_attn_matvec_f32 with k = 1, but without
+ * a workspace: it is for callers that hold device buffers yet cannot allocate
+ * device memory (a host that only receives buffers from another framework's
+ * allocator, or a loop where cudaMalloc's implicit synchronisation and pool
+ * growth are not allowed).  Its scratch is a fixed array of
+ * LAKER_NOALLOC_SCRATCH_BYTES inside the library, held by every GPU that loads
+ * it until the process exits; m must not exceed LAKER_NOALLOC_MAX_ROWS
+ * (LAKER_ERR_SCRATCH_LIMIT otherwise).  The first call on each device sets the
+ * array up (symbol lookup, possibly loading the module): make it before any
+ * stream capture.  Every call reuses the same array, so calls that overlap on
+ * the GPU (other streams, unordered host threads) race.  It calls no
+ * allocation routine.  This entry point has no counterpart in the reference. */
+#define LAKER_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+#define LAKER_NOALLOC_MAX_ROWS 2000000
+int laker_attn_matvec_f32_noalloc(const float* rows32, int64_t m, const float* cols32, int64_t n,
+                                  int d, float lam, int clamp, const float* x, float* y,
+                                  void* stream);
 
 /* FP64 fused matvec / residual ("accurate" operator: FP64 logits, FP64 exp,
  * FP64 accumulation).

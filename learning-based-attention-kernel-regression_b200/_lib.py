@@ -32,6 +32,7 @@ LAKER_ERR_NONFINITE = 5
 LAKER_ERR_TIMEOUT = 6
 LAKER_ERR_WORKSPACE = 7
 LAKER_ERR_UNSUPPORTED = 8
+LAKER_ERR_SCRATCH_LIMIT = 9
 
 
 class LakerError(RuntimeError):
@@ -106,6 +107,10 @@ _SIGNATURES = {
         c_int,
         [_P, c_int64, _P, c_int64, c_int, c_float, c_int, _P, c_int, c_int64, _P, c_int64, _P,
          c_size_t, _P],
+    ),
+    "laker_attn_matvec_f32_noalloc": (
+        c_int,
+        [_P, c_int64, _P, c_int64, c_int, c_float, c_int, _P, _P, _P],
     ),
     "laker_attn_matvec_f64": (
         c_int,
