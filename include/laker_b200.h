@@ -100,6 +100,14 @@ int laker_attn_matvec_f32(const float* rows32, int64_t m, const float* cols32, i
                           float lam, int clamp, const float* X, int k, int64_t ldx, float* Y,
                           int64_t ldy, void* workspace, size_t workspace_bytes, void* stream);
 
+/* Algorithmic work of one square FP32 operator application (the kernel
+ * laker_attn_matvec_f32 and laker_pcg_solve use for n points of dimension d):
+ * kernel entries evaluated, FP32 flops (2 per FMA: d logit FMAs plus one
+ * accumulation FMA per use of an entry) and exp2 evaluations.  With the
+ * symmetric kernel each off-diagonal entry is evaluated once and used twice.
+ * No counterpart in the reference (roofline accounting). */
+int laker_fp32_matvec_work(int64_t n, int d, double* entries, double* flops, double* exps);
+
 /* Allocation-free FP32 fused matvec (single right-hand side).
  *   y = lam * x[:m] + exp(Er Ec^T) x          (x: n, y: m)
  * Same arguments and result as laker_attn_matvec_f32 with k = 1, but without

@@ -134,6 +134,10 @@ _SIGNATURES = {
         c_int,
         [_P, c_int64, c_int, _P, _P, c_int64, c_int64, _P, _P],
     ),
+    "laker_fp32_matvec_work": (
+        c_int,
+        [c_int64, c_int, POINTER(c_double), POINTER(c_double), POINTER(c_double)],
+    ),
     "laker_peaks_scratch_bytes": (c_size_t, []),
     "laker_measure_peaks": (
         c_int,
@@ -357,6 +361,14 @@ def variance_finalize(q64, m, d, Kxq, V) -> torch.Tensor:
         "laker_variance_finalize",
     )
     return var
+
+
+def fp32_matvec_work(n: int, d: int) -> dict:
+    """Entries evaluated, FP32 flops and exp2s of one square FP32 operator application."""
+    e, f, x = c_double(), c_double(), c_double()
+    check(load().laker_fp32_matvec_work(n, d, ctypes.byref(e), ctypes.byref(f), ctypes.byref(x)),
+          "laker_fp32_matvec_work")
+    return {"entries": e.value, "flops": f.value, "exps": x.value}
 
 
 def measure_peaks(device: torch.device) -> dict:

@@ -14,6 +14,7 @@
 #include <cstdlib>
 
 #include "internal.cuh"
+#include "sym.cuh"
 
 namespace laker {
 namespace {
@@ -449,7 +450,13 @@ extern "C" size_t laker_matvec_workspace_bytes(int64_t m, int64_t n, int d, int 
   if (m < 0 || n < 0 || d < 1 || d > 16 || k < 1) return 0;
   if (k > 1) return kWsHeader;
   const SegPlan p = precision == 64 ? k4_plan(m, n, d) : k1_plan(m, n, d);
-  return kWsHeader + (size_t)p.S * (size_t)m * sizeof(double);
+  size_t bytes = (size_t)p.S * (size_t)m * sizeof(double);
+  if (precision != 64 && m == n && n > 0) {
+    // a square product with the same embeddings may take the symmetric kernel
+    const size_t sym = sym_partial_bytes(k1s_plan(n, d));
+    if (sym > bytes) bytes = sym;
+  }
+  return kWsHeader + bytes;
 }
 
 extern "C" int laker_attn_matvec_f32(const float* rows32, int64_t m, const float* cols32, int64_t n,
@@ -471,8 +478,19 @@ extern "C" int laker_attn_matvec_f32(const float* rows32, int64_t m, const float
   }
   // Single RHS: strided x is staged element-wise; a contiguous copy is not needed.
   if (ldx != 1) return LAKER_ERR_UNSUPPORTED;
+  char* wbase = static_cast<char*>(workspace) + kWsHeader;
+  if (rows32 == cols32 && m == n && k1_use_symmetric()) {
+    // the operator itself: every off-diagonal entry evaluated once
+    const SymPlan sp = k1s_plan(n, d);
+    double* rowpart = reinterpret_cast<double*>(wbase);
+    float* colpart = reinterpret_cast<float*>(
+        wbase + round_up((int64_t)(sym_rowpart_elems(sp) * sizeof(double)), 256));
+    e = launch_k1s(cols32, n, d, clamp, X, rowpart, colpart, sp, &hdr->status, nullptr, s);
+    if (e == cudaSuccess) e = launch_sym_finish(sp, rowpart, colpart, n, lam, X, Y, ldy, s);
+    return e == cudaSuccess ? LAKER_OK : fail_cuda(e);
+  }
   const SegPlan plan = k1_plan(m, n, d);
-  double* part = reinterpret_cast<double*>(static_cast<char*>(workspace) + kWsHeader);
+  double* part = reinterpret_cast<double*>(wbase);
   if (n > 0) {
     e = launch_k1(rows32, m, cols32, n, d, clamp, X, part, plan, &hdr->status, nullptr, s);
     if (e != cudaSuccess) return fail_cuda(e);

@@ -16,6 +16,7 @@
 // the solve has finished, so the host can launch several iterations between
 // status polls.
 #include "pcg_state.cuh"
+#include "sym.cuh"
 
 namespace laker {
 int precond_grid();
@@ -65,9 +66,13 @@ __global__ void __launch_bounds__(T)
   }
 }
 
-// Ap = lam p + sum_s part[s]; p.Ap, p.p, Ap.Ap -> breakdown test and alpha.
+// Ap = lam p + (partial sums of the FP32 matvec); p.Ap, p.p, Ap.Ap ->
+// breakdown test and alpha.  SYM: partials of the symmetric kernel (row runs
+// in `part`, column sums in `colpart`), else S column-segment partials.
+template <bool SYM>
 __global__ void __launch_bounds__(T)
-    pcg_after_matvec_kernel(const double* __restrict__ part, int S, const float* __restrict__ p,
+    pcg_after_matvec_kernel(const double* __restrict__ part, int S, SymPlan sp,
+                            const float* __restrict__ colpart, const float* __restrict__ p,
                             float* __restrict__ Ap, int64_t n, double* blockpart, PcgState* st) {
   if (st->done) return;
   __shared__ double s_red[3 * (T / 32)];
@@ -76,7 +81,11 @@ __global__ void __launch_bounds__(T)
   for (int64_t i = blockIdx.x * (int64_t)T + threadIdx.x; i < n; i += (int64_t)gridDim.x * T) {
     const double pi = p[i];
     double a = lam * pi;
-    for (int s = 0; s < S; ++s) a += part[(int64_t)s * n + i];
+    if (SYM) {
+      a += sym_row_sum(sp, part, colpart, i);
+    } else {
+      for (int s = 0; s < S; ++s) a += part[(int64_t)s * n + i];
+    }
     const float af = (float)a;
     Ap[i] = af;
     d0 = fma(pi, (double)af, d0);
@@ -305,7 +314,12 @@ PcgWs carve(void* base, int64_t n, int d, int nr) {
   w.Ap = reinterpret_cast<float*>(take(n * sizeof(float)));
   w.z = reinterpret_cast<float*>(take(n * sizeof(float)));
   w.p = reinterpret_cast<float*>(take(n * sizeof(float)));
-  w.part32 = reinterpret_cast<double*>(take((size_t)p1.S * n * sizeof(double)));
+  {
+    // FP32 matvec partials: column segments, or the symmetric kernel's layout
+    size_t b32 = (size_t)p1.S * n * sizeof(double);
+    const size_t bs = sym_partial_bytes(k1s_plan(n, d));
+    w.part32 = reinterpret_cast<double*>(take(b32 > bs ? b32 : bs));
+  }
   w.part64 = reinterpret_cast<double*>(take((size_t)p4.S * n * sizeof(double)));
   w.blockpart = reinterpret_cast<double*>(take((size_t)G * 4 * sizeof(double)));
   (void)nr;  // the apply's partials are sized for the largest padded row (1024)
@@ -342,6 +356,11 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   PcgWs w = carve(workspace, n, d, nr);
   const SegPlan p1 = k1_plan(n, n, d), p4 = k4_plan(n, n, d);
+  const bool sym = k1_use_symmetric();
+  const SymPlan sp = k1s_plan(n, d);
+  float* sym_col = reinterpret_cast<float*>(
+      reinterpret_cast<char*>(w.part32) +
+      round_up((int64_t)(sym_rowpart_elems(sp) * sizeof(double)), 256));
   const int G = vec_grid(n), Gp = precond_grid();
   const PcView view{pc ? pc->q_basis : nullptr, pc ? pc->w_core : nullptr, n, nr,
                     pc ? pc->ldq : 4, pc ? pc->inv_sqrt_iso : 1.0};
@@ -421,10 +440,20 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
     const int chunk = (prm->max_iter - launched) < check ? (prm->max_iter - launched) : check;
     for (int c = 0; c < chunk; ++c) {
       t32.begin(s);
-      launch_k1(op->packed32, n, op->packed32, n, d, op->clamp, w.p, w.part32, p1, dstatus,
-                &w.st->active, s);
+      if (sym) {
+        launch_k1s(op->packed32, n, d, op->clamp, w.p, w.part32, sym_col, sp, dstatus,
+                   &w.st->active, s);
+      } else {
+        launch_k1(op->packed32, n, op->packed32, n, d, op->clamp, w.p, w.part32, p1, dstatus,
+                  &w.st->active, s);
+      }
       t32.end(s);
-      pcg_after_matvec_kernel<<<G, T, 0, s>>>(w.part32, p1.S, w.p, w.Ap, n, w.blockpart, w.st);
+      if (sym)
+        pcg_after_matvec_kernel<true><<<G, T, 0, s>>>(w.part32, 0, sp, sym_col, w.p, w.Ap, n,
+                                                      w.blockpart, w.st);
+      else
+        pcg_after_matvec_kernel<false><<<G, T, 0, s>>>(w.part32, p1.S, sp, nullptr, w.p, w.Ap, n,
+                                                       w.blockpart, w.st);
       pcg_update_xr_kernel<<<G, T, 0, s>>>(w.p, w.Ap, X, w.r, n, w.blockpart, w.st);
       t64.begin(s);
       launch_k4(op->packed64, n, op->packed64, n, d, op->clamp, X, w.part64, p4, dstatus,

@@ -66,7 +66,7 @@ class PreconditionedConjugateGradient:
         restart_freq: Optional[int] = None,
         breakdown_eps: Optional[float] = None,
         autograd_safe: bool = False,
-        reliable_delta: float = 0.05,
+        reliable_delta: float = 0.03,
         check_every: int = 0,
         profile: bool = False,
     ) -> None:
