@@ -228,6 +228,45 @@ int laker_pcg_solve(const laker_operator* op, const laker_precond* pc, const dou
                     size_t workspace_bytes, laker_pcg_result* result, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Batched PCG: many independent regressions in one solve                    */
+/* ------------------------------------------------------------------------ */
+/* Instance k has n[k] points; every batched vector and packed buffer holds
+ * instance k at points [offsets[k], offsets[k] + n[k]) with offsets[0] = 0 and
+ * offsets[k+1] = offsets[k] + round_up(n[k], 256) (zero padding between).
+ * laker_batch_layout fills offsets[0..count] (host array) and returns the
+ * total padded length. */
+int64_t laker_batch_layout(int count, const int64_t* n, int64_t* offsets);
+
+typedef struct laker_batch {
+  int count;                    /* instances                                   */
+  int d;                        /* embedding dimension (all instances)         */
+  int clamp;                    /* 1: clamp Gram entries (see attn_matvec)     */
+  const int64_t* n;             /* HOST [count]: points per instance (>= 1)    */
+  const double* lambda_reg;     /* HOST [count]                                */
+  const float* packed32;        /* DEVICE: packed32 of instance k at float
+                                   offset offsets[k] * round_up(d, 2)          */
+  const double* packed64;       /* DEVICE: packed64 of instance k at double
+                                   offset offsets[k] * round_up(d, 2)          */
+  const laker_precond* precond; /* HOST [count] (device factors) or NULL       */
+} laker_batch;
+
+size_t laker_pcg_batched_workspace_bytes(int count, const int64_t* n, int d);
+
+/* Solves A_k x_k = b_k for every instance with the mixed-precision PCG of
+ * laker_pcg_solve in one device loop: one symmetric FP32 matvec launch covers
+ * all unconverged instances (block-diagonal pair list), every other step runs
+ * one CTA per instance, per-instance scalars and convergence masks live on the
+ * device, and the iteration is captured once as a CUDA graph and replayed
+ * until every instance has stopped.  B, X: batched vectors (padded length).
+ * results: HOST array of count results.  Returns LAKER_OK unless a call
+ * failed; per-instance outcomes are in results[k].status.
+ * Replaces a loop of PreconditionedConjugateGradient.solve calls
+ * (laker/solvers.py:130-295) over independent problems. */
+int laker_pcg_solve_batched(const laker_batch* batch, const double* B, double* X,
+                            const laker_pcg_params* params, void* workspace,
+                            size_t workspace_bytes, laker_pcg_result* results, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Predictive variance                                                       */
 /* ------------------------------------------------------------------------ */
 /* var_q = max(0, exp(||e_q||^2) - sum_i Kxq[i, q] * V[i, q]) for q < m, with

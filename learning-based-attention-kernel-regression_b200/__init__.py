@@ -26,6 +26,7 @@ from .kernels import AttentionKernelOperator, KernelOperator
 from .models import LAKERRegressor
 from .preconditioner import CCCPPreconditioner, adaptive_shrinkage_rho, eigh_stable
 from .solvers import PreconditionedConjugateGradient
+from .batched import BatchedPCG, build_cccp_batched
 
 __version__ = "0.1.0"
 
@@ -39,6 +40,8 @@ def build(force: bool = False, verbose: bool = False):
 
 __all__ = [
     "AttentionKernelOperator",
+    "BatchedPCG",
+    "build_cccp_batched",
     "CCCPPreconditioner",
     "KernelOperator",
     "LAKERCore",

@@ -93,8 +93,28 @@ class laker_pcg_result(ctypes.Structure):
     ]
 
 
+class laker_batch(ctypes.Structure):
+    _fields_ = [
+        ("count", c_int),
+        ("d", c_int),
+        ("clamp", c_int),
+        ("n", POINTER(c_int64)),
+        ("lambda_reg", POINTER(c_double)),
+        ("packed32", c_void_p),
+        ("packed64", c_void_p),
+        ("precond", POINTER(laker_precond)),
+    ]
+
+
 _P = c_void_p
 _SIGNATURES = {
+    "laker_batch_layout": (c_int64, [c_int, POINTER(c_int64), POINTER(c_int64)]),
+    "laker_pcg_batched_workspace_bytes": (c_size_t, [c_int, POINTER(c_int64), c_int]),
+    "laker_pcg_solve_batched": (
+        c_int,
+        [POINTER(laker_batch), _P, _P, POINTER(laker_pcg_params), _P, c_size_t,
+         POINTER(laker_pcg_result), _P],
+    ),
     "laker_version": (c_int, []),
     "laker_status_string": (ctypes.c_char_p, [c_int]),
     "laker_last_cuda_error": (c_int, []),

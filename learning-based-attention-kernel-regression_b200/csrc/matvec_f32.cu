@@ -482,9 +482,8 @@ extern "C" int laker_attn_matvec_f32(const float* rows32, int64_t m, const float
   if (rows32 == cols32 && m == n && k1_use_symmetric()) {
     // the operator itself: every off-diagonal entry evaluated once
     const SymPlan sp = k1s_plan(n, d);
-    double* rowpart = reinterpret_cast<double*>(wbase);
-    float* colpart = reinterpret_cast<float*>(
-        wbase + round_up((int64_t)(sym_rowpart_elems(sp) * sizeof(double)), 256));
+    float* rowpart = reinterpret_cast<float*>(wbase);
+    float* colpart = sym_colpart_ptr(wbase, sp);
     e = launch_k1s(cols32, n, d, clamp, X, rowpart, colpart, sp, &hdr->status, nullptr, s);
     if (e == cudaSuccess) e = launch_sym_finish(sp, rowpart, colpart, n, lam, X, Y, ldy, s);
     return e == cudaSuccess ? LAKER_OK : fail_cuda(e);

@@ -11,10 +11,15 @@
 // sums take one packed FMA (as in the plain kernel) and -- for a < b -- the
 // column sums another one.  Column sums are reduced over the warp with
 // shuffles and over the CTA in shared memory, then stored per pair; row sums
-// are kept across the consecutive pairs of one row block and stored once per
-// (CTA, row block) run.  A fixed-order finish adds both partial sets, so the
-// result is deterministic.  Work per computed entry: d FMA + 2 FMA + 1 exp2,
+// are accumulated over the pair's column tiles and also stored per pair.  A
+// fixed-order finish adds both partial sets, so the result is deterministic
+// and does not depend on the grid, on the CTA that processed a pair or on the
+// other instances of a batch.  Work per computed entry: d FMA + 2 FMA + 1 exp2,
 // i.e. (d + 2) / 2 FMA and 1/2 exp2 per logical entry.
+//
+// The BATCHED instantiation runs many independent problems in one launch
+// (BatchMap): the pair list is the concatenation of the instances' pair
+// lists, so the operator is block diagonal; converged instances are skipped.
 #include <cstdlib>
 
 #include "sym.cuh"
@@ -22,11 +27,84 @@
 namespace laker {
 namespace {
 
-template <int DP, int R, int T, bool CLAMP>
+// Position in a CTA's flat sequence of column tiles (pair p, tile t of block b).
+struct SymCursor {
+  int64_t p, p_end;
+  int inst;
+  int64_t a, b;
+  int t;
+  // metadata of instance `inst`
+  int64_t nb, npts, seg, blk0, pstart, pend;
+};
+
+template <bool BATCHED>
+__device__ __forceinline__ void cursor_load_inst(SymCursor& cu, const SymPlan& sp,
+                                                 const BatchMap& bm, int64_t n) {
+  if (BATCHED) {
+    cu.nb = bm.nblk[cu.inst];
+    cu.npts = bm.npts[cu.inst];
+    cu.seg = bm.seg[cu.inst];
+    cu.blk0 = bm.blk_start[cu.inst];
+    cu.pstart = bm.pair_start[cu.inst];
+    cu.pend = bm.pair_start[cu.inst + 1];
+  } else {
+    cu.nb = sp.nb;
+    cu.npts = n;
+    cu.seg = 0;
+    cu.blk0 = 0;
+    cu.pstart = 0;
+    cu.pend = sp.npairs;
+  }
+}
+
+// Place the cursor on tile 0 of pair p, moving past finished instances.
+// Returns false when the CTA's range is exhausted.
+template <bool BATCHED>
+__device__ __forceinline__ bool cursor_settle(SymCursor& cu, const SymPlan& sp, const BatchMap& bm,
+                                              int64_t n) {
+  for (;;) {
+    if (cu.p >= cu.p_end) return false;
+    if (BATCHED) {
+      while (cu.p >= cu.pend) {
+        ++cu.inst;
+        cursor_load_inst<BATCHED>(cu, sp, bm, n);
+      }
+      if (bm.done && bm.done[cu.inst]) {
+        cu.p = cu.pend;
+        continue;
+      }
+    }
+    sym_pair_coords(cu.p - cu.pstart, cu.nb, &cu.a, &cu.b);
+    cu.t = 0;
+    return true;
+  }
+}
+
+// Next tile that holds points (tiles starting at or past the instance's n are
+// empty and skipped).
+template <bool BATCHED, int B, int TC, int TPB>
+__device__ __forceinline__ bool cursor_next(SymCursor& cu, const SymPlan& sp, const BatchMap& bm,
+                                            int64_t n) {
+  ++cu.t;
+  if (cu.t < TPB && cu.b * B + (int64_t)cu.t * TC < cu.npts) return true;
+  ++cu.p;
+  if (cu.p >= cu.p_end) return false;
+  if (cu.p < cu.pend) {
+    if (++cu.b >= cu.nb) {
+      ++cu.a;
+      cu.b = cu.a;
+    }
+    cu.t = 0;
+    return true;
+  }
+  return cursor_settle<BATCHED>(cu, sp, bm, n);
+}
+
+template <int DP, int R, int T, bool CLAMP, bool BATCHED>
 __global__ void __launch_bounds__(T, 3)
     k1s_matvec_f32(const float* __restrict__ E, int64_t n, const float* __restrict__ x,
-                   float* __restrict__ colpart, double* __restrict__ rowpart, SymPlan sp,
-                   int* status, const int* gate) {
+                   float* __restrict__ colpart, float* __restrict__ rowpart, SymPlan sp,
+                   BatchMap bm, int* status, const int* gate) {
   if (gate && *gate == 0) return;
   constexpr int TC = kTileCols32;
   constexpr int TP = TC / 2;
@@ -46,11 +124,22 @@ __global__ void __launch_bounds__(T, 3)
   const int64_t p_end = p_begin + sp.q + (c < sp.rem ? 1 : 0);
   if (p_begin >= p_end) return;
 
-  // ---- the CTA's flat tile sequence: (pair, tile-in-block), skipping tiles
-  // that start at or beyond n (they hold no points).
-  auto tile_col0 = [&](int64_t b, int t) -> int64_t { return b * B + (int64_t)t * TC; };
-  int64_t a0, b0;
-  sym_pair_coords(p_begin, sp.nb, &a0, &b0);
+  // consumer cursor (cu) and prefetch cursor (nx) over the same tile sequence
+  SymCursor cu;
+  cu.p = p_begin;
+  cu.p_end = p_end;
+  cu.inst = 0;
+  if (BATCHED) {
+    // instance of the first pair: binary search of pair_start
+    int lo = 0, hi = bm.count - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (bm.pair_start[mid] <= p_begin) lo = mid; else hi = mid - 1;
+    }
+    cu.inst = lo;
+  }
+  cursor_load_inst<BATCHED>(cu, sp, bm, n);
+  if (!cursor_settle<BATCHED>(cu, sp, bm, n)) return;  // uniform: every thread sees the same
 
   if (tid == 0) {
     mbar_init(&bar[0], 1);
@@ -59,48 +148,28 @@ __global__ void __launch_bounds__(T, 3)
   }
   __syncthreads();
 
+  auto col0_of = [&](const SymCursor& s) -> int64_t { return s.seg + s.b * B + (int64_t)s.t * TC; };
   auto issue = [&](int64_t col0, int buf) {
     mbar_arrive_expect_tx(&bar[buf], TILE_FLOATS * 4);
     bulk_g2s(sE[buf], E + (col0 >> 1) * (DP * 2), TILE_FLOATS * 4, &bar[buf]);
   };
-  auto load_x = [&](int64_t col0, int buf) {
-    for (int j = tid; j < TC; j += T) {
-      const int64_t cc = col0 + j;
-      sX[buf][j] = (cc < n) ? x[cc] : 0.0f;
-    }
+  auto load_x = [&](const SymCursor& s, int buf) {
+    const int64_t local0 = s.b * B + (int64_t)s.t * TC;
+    for (int j = tid; j < TC; j += T) sX[buf][j] = (local0 + j < s.npts) ? x[s.seg + local0 + j] : 0.0f;
   };
 
-  // iteration state: current pair (pa, pb), tile t within block pb
-  int64_t pa = a0, pb = b0, p = p_begin;
-  int t = 0;
-  // next-tile cursor for prefetching
-  int64_t na = a0, nbk = b0, np = p_begin;
-  int nt = 0;
-  auto advance = [&](int64_t& qa, int64_t& qb, int64_t& qp, int& qt) {
-    // move to the next valid tile of the sequence
-    for (;;) {
-      if (++qt >= TPB || tile_col0(qb, qt) >= n) {
-        qt = 0;
-        ++qp;
-        if (qp >= p_end) return;
-        if (++qb >= sp.nb) {
-          ++qa;
-          qb = qa;
-        }
-      }
-      if (tile_col0(qb, qt) < n) return;
-    }
-  };
-
-  // rows of block pa in registers
+  // rows of block (cu.inst, cu.a) in registers; row sums of the current pair
   float2 ev[R][DP];
   float2 xr[R];
   double acc[R];
-  auto load_rows = [&](int64_t a) {
+#pragma unroll
+  for (int r = 0; r < R; ++r) acc[r] = 0.0;
+  auto load_rows = [&](const SymCursor& s) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int64_t i = a * B + r * T + tid;
-      const bool ok = i < n;
+      const int64_t li = s.a * B + r * T + tid;
+      const bool ok = li < s.npts;
+      const int64_t i = s.seg + li;
       const float* blk = E + (i >> 1) * (DP * 2) + (i & 1);
 #pragma unroll
       for (int k = 0; k < DP; ++k) {
@@ -109,31 +178,34 @@ __global__ void __launch_bounds__(T, 3)
       }
       const float xi = ok ? x[i] : 0.0f;
       xr[r] = make_float2(xi, xi);
+    }
+  };
+  // Row sums are stored per pair: the finish then adds an instance's pairs in
+  // a fixed order that does not depend on which CTA processed them (the
+  // result is the same alone or inside any batch).
+  auto flush_rows = [&](int64_t pair) {
+    float* dst = rowpart + pair * (int64_t)B;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      dst[r * T + tid] = (float)acc[r];
       acc[r] = 0.0;
     }
   };
-  auto flush_rows = [&](int64_t a) {
-    double* dst = rowpart + (c + a) * (int64_t)B;
-#pragma unroll
-    for (int r = 0; r < R; ++r) dst[r * T + tid] = acc[r];
-  };
 
-  load_rows(pa);
-  // first tile
-  if (tid == 0) issue(tile_col0(nbk, nt), 0);
-  load_x(tile_col0(nbk, nt), 0);
-  advance(na, nbk, np, nt);
+  load_rows(cu);
+  SymCursor nx = cu;
+  if (tid == 0) issue(col0_of(nx), 0);
+  load_x(nx, 0);
+  bool have_nx = cursor_next<BATCHED, B, TC, TPB>(nx, sp, bm, n);
   __syncthreads();
 
   int k_tile = 0, issued = 1, consumed = 0;
   bool failed = false;
-  while (p < p_end) {
+  for (;;) {
     const int buf = k_tile & 1;
-    const bool have_next = np < p_end;
-    if (have_next) {
-      const int64_t col0 = tile_col0(nbk, nt);
-      if (tid == 0) issue(col0, buf ^ 1);
-      load_x(col0, buf ^ 1);
+    if (have_nx) {
+      if (tid == 0) issue(col0_of(nx), buf ^ 1);
+      load_x(nx, buf ^ 1);
       ++issued;
     }
     const int ok = __syncthreads_and(mbar_wait_bounded(&bar[buf], (k_tile >> 1) & 1, status) ? 1 : 0);
@@ -142,7 +214,7 @@ __global__ void __launch_bounds__(T, 3)
       break;
     }
     ++consumed;
-    const bool offdiag = pa != pb;
+    const bool offdiag = cu.a != cu.b;
     const float* Et = sE[buf];
     const float2* X2 = reinterpret_cast<const float2*>(sX[buf]);
     float2 tacc[R];
@@ -235,33 +307,25 @@ __global__ void __launch_bounds__(T, 3)
     for (int r = 0; r < R; ++r) acc[r] += (double)tacc[r].x + (double)tacc[r].y;
     __syncthreads();  // sE/sX[buf] are refilled next; sCol is complete
     if (offdiag) {
-      // this tile's column sums (columns t*TC .. t*TC+TC-1 of block pb)
+      // this tile's column sums (columns t*TC .. t*TC+TC-1 of block b)
       for (int j = tid; j < TC; j += T) {
         float s = 0.0f;
 #pragma unroll
         for (int w = 0; w < NW; ++w) s += sCol[w][j];
-        colpart[sym_pair_index(pa, pb, sp.nb) * (int64_t)B + t * TC + j] = s;
+        colpart[cu.p * (int64_t)B + cu.t * TC + j] = s;
       }
     }
     __syncthreads();  // sCol is reused by the next tile
 
-    // advance the consumer cursor
-    const int64_t prev_a = pa;
+    // advance the consumer; store the row sums when the pair changes and
+    // reload the rows when the row block changes
+    const int64_t prev_pair = cu.p, prev_block = cu.blk0 + cu.a;
+    const bool more = cursor_next<BATCHED, B, TC, TPB>(cu, sp, bm, n);
     ++k_tile;
-    {
-      int64_t qa = pa, qb = pb, qp = p;
-      int qt = t;
-      advance(qa, qb, qp, qt);
-      pa = qa;
-      pb = qb;
-      p = qp;
-      t = qt;
-    }
-    if (p >= p_end || pa != prev_a) {
-      flush_rows(prev_a);
-      if (p < p_end) load_rows(pa);
-    }
-    if (have_next) advance(na, nbk, np, nt);
+    if (!more || cu.p != prev_pair) flush_rows(prev_pair);
+    if (more && cu.blk0 + cu.a != prev_block) load_rows(cu);
+    if (!more) break;
+    if (have_nx) have_nx = cursor_next<BATCHED, B, TC, TPB>(nx, sp, bm, n);
   }
   if (failed) {
     for (int k = consumed + 1; k < issued; ++k) mbar_wait_bounded(&bar[k & 1], (k >> 1) & 1, status);
@@ -277,12 +341,12 @@ namespace {
 constexpr int kSymRows = 4;      // rows per thread
 constexpr int kSymThreads = 128;  // threads per CTA -> B = 512 points per block
 
-template <int DP, bool CLAMP>
-cudaError_t launch_k1s_t(const float* E, int64_t n, const float* x, double* rowpart,
-                         float* colpart, const SymPlan& sp, int* status, const int* gate,
-                         cudaStream_t s) {
-  k1s_matvec_f32<DP, kSymRows, kSymThreads, CLAMP>
-      <<<sp.grid, kSymThreads, 0, s>>>(E, n, x, colpart, rowpart, sp, status, gate);
+template <int DP, bool CLAMP, bool BATCHED>
+cudaError_t launch_k1s_t(const float* E, int64_t n, const float* x, float* rowpart,
+                         float* colpart, const SymPlan& sp, const BatchMap& bm, int* status,
+                         const int* gate, cudaStream_t s) {
+  k1s_matvec_f32<DP, kSymRows, kSymThreads, CLAMP, BATCHED>
+      <<<sp.grid, kSymThreads, 0, s>>>(E, n, x, colpart, rowpart, sp, bm, status, gate);
   return cudaGetLastError();
 }
 
@@ -292,8 +356,9 @@ int k1s_occupancy(int dp) {
   int& c = cache[dp / 2];
   if (c > 0) return c;
   const void* fn = nullptr;
-#define LAKER_K1S_FN(DPv) \
-  if (dp == DPv) fn = reinterpret_cast<const void*>(&k1s_matvec_f32<DPv, kSymRows, kSymThreads, false>);
+#define LAKER_K1S_FN(DPv)                                                                 \
+  if (dp == DPv)                                                                          \
+    fn = reinterpret_cast<const void*>(&k1s_matvec_f32<DPv, kSymRows, kSymThreads, false, false>);
   LAKER_K1S_FN(2) LAKER_K1S_FN(4) LAKER_K1S_FN(6) LAKER_K1S_FN(8) LAKER_K1S_FN(10) LAKER_K1S_FN(12)
   LAKER_K1S_FN(14) LAKER_K1S_FN(16)
 #undef LAKER_K1S_FN
@@ -320,39 +385,7 @@ int k1s_occupancy(int dp) {
     default: return cudaErrorInvalidValue;              \
   }
 
-}  // namespace
-
-SymPlan k1s_plan(int64_t n, int d) {
-  SymPlan sp{};
-  sp.B = kSymRows * kSymThreads;
-  sp.nb = n > 0 ? ceil_div(n, sp.B) : 1;
-  sp.npairs = sp.nb * (sp.nb + 1) / 2;
-  const int64_t slots = (int64_t)sm_count() * k1s_occupancy(padded_dim(d));
-  sp.grid = (int)(sp.npairs < slots ? sp.npairs : slots);
-  sp.q = sp.npairs / sp.grid;
-  sp.rem = sp.npairs % sp.grid;
-  sp.cfg = 0;
-  return sp;
-}
-
-cudaError_t launch_k1s(const float* E32, int64_t n, int d, int clamp, const float* x,
-                       double* rowpart, float* colpart, const SymPlan& sp, int* status,
-                       const int* gate, cudaStream_t s) {
-  const int dp = padded_dim(d);
-  if (clamp) {
-    LAKER_DISPATCH_DPS(dp, return (launch_k1s_t<DPv, true>(E32, n, x, rowpart, colpart, sp, status, gate, s)));
-  } else {
-    LAKER_DISPATCH_DPS(dp, return (launch_k1s_t<DPv, false>(E32, n, x, rowpart, colpart, sp, status, gate, s)));
-  }
-  return cudaErrorInvalidValue;
-}
-
-}  // namespace laker
-
-namespace laker {
-namespace {
-
-__global__ void sym_finish_kernel(SymPlan sp, const double* __restrict__ rowpart,
+__global__ void sym_finish_kernel(SymPlan sp, const float* __restrict__ rowpart,
                                   const float* __restrict__ colpart, int64_t n, float lam,
                                   const float* __restrict__ x, float* __restrict__ y, int64_t ldy) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
@@ -362,7 +395,53 @@ __global__ void sym_finish_kernel(SymPlan sp, const double* __restrict__ rowpart
 
 }  // namespace
 
-cudaError_t launch_sym_finish(const SymPlan& sp, const double* rowpart, const float* colpart,
+int sym_block_points() { return kSymRows * kSymThreads; }
+
+SymPlan k1s_plan_pairs(int64_t nb, int64_t npairs, int d) {
+  SymPlan sp{};
+  sp.B = kSymRows * kSymThreads;
+  sp.nb = nb;
+  sp.npairs = npairs;
+  const int64_t slots = (int64_t)sm_count() * k1s_occupancy(padded_dim(d));
+  sp.grid = (int)(npairs < slots ? (npairs > 0 ? npairs : 1) : slots);
+  sp.q = npairs / sp.grid;
+  sp.rem = npairs % sp.grid;
+  sp.cfg = 0;
+  return sp;
+}
+
+SymPlan k1s_plan(int64_t n, int d) {
+  const int B = kSymRows * kSymThreads;
+  const int64_t nb = n > 0 ? ceil_div(n, B) : 1;
+  return k1s_plan_pairs(nb, nb * (nb + 1) / 2, d);
+}
+
+cudaError_t launch_k1s(const float* E32, int64_t n, int d, int clamp, const float* x,
+                       float* rowpart, float* colpart, const SymPlan& sp, int* status,
+                       const int* gate, cudaStream_t s) {
+  const int dp = padded_dim(d);
+  const BatchMap none{};
+  if (clamp) {
+    LAKER_DISPATCH_DPS(dp, return (launch_k1s_t<DPv, true, false>(E32, n, x, rowpart, colpart, sp, none, status, gate, s)));
+  } else {
+    LAKER_DISPATCH_DPS(dp, return (launch_k1s_t<DPv, false, false>(E32, n, x, rowpart, colpart, sp, none, status, gate, s)));
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_k1s_batched(const float* E32, int d, int clamp, const float* x,
+                               float* rowpart, float* colpart, const SymPlan& sp,
+                               const BatchMap& bm, int* status, const int* gate, cudaStream_t s) {
+  const int dp = padded_dim(d);
+  if (clamp) {
+    LAKER_DISPATCH_DPS(dp, return (launch_k1s_t<DPv, true, true>(E32, 0, x, rowpart, colpart, sp, bm, status, gate, s)));
+  } else {
+    LAKER_DISPATCH_DPS(dp, return (launch_k1s_t<DPv, false, true>(E32, 0, x, rowpart, colpart, sp, bm, status, gate, s)));
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_sym_finish(const SymPlan& sp, const float* rowpart, const float* colpart,
                               int64_t n, float lam, const float* x, float* y, int64_t ldy,
                               cudaStream_t s) {
   int g = (int)ceil_div(n, 256);

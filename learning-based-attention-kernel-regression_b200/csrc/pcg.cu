@@ -67,11 +67,12 @@ __global__ void __launch_bounds__(T)
 }
 
 // Ap = lam p + (partial sums of the FP32 matvec); p.Ap, p.p, Ap.Ap ->
-// breakdown test and alpha.  SYM: partials of the symmetric kernel (row runs
-// in `part`, column sums in `colpart`), else S column-segment partials.
+// breakdown test and alpha.  SYM: per-pair row and column sums of the
+// symmetric kernel, else S column-segment partials in `part`.
 template <bool SYM>
 __global__ void __launch_bounds__(T)
     pcg_after_matvec_kernel(const double* __restrict__ part, int S, SymPlan sp,
+                            const float* __restrict__ rowpart,
                             const float* __restrict__ colpart, const float* __restrict__ p,
                             float* __restrict__ Ap, int64_t n, double* blockpart, PcgState* st) {
   if (st->done) return;
@@ -82,7 +83,7 @@ __global__ void __launch_bounds__(T)
     const double pi = p[i];
     double a = lam * pi;
     if (SYM) {
-      a += sym_row_sum(sp, part, colpart, i);
+      a += sym_row_sum(sp, rowpart, colpart, i);
     } else {
       for (int s = 0; s < S; ++s) a += part[(int64_t)s * n + i];
     }
@@ -358,9 +359,8 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
   const SegPlan p1 = k1_plan(n, n, d), p4 = k4_plan(n, n, d);
   const bool sym = k1_use_symmetric();
   const SymPlan sp = k1s_plan(n, d);
-  float* sym_col = reinterpret_cast<float*>(
-      reinterpret_cast<char*>(w.part32) +
-      round_up((int64_t)(sym_rowpart_elems(sp) * sizeof(double)), 256));
+  float* sym_row = reinterpret_cast<float*>(w.part32);
+  float* sym_col = sym_colpart_ptr(w.part32, sp);
   const int G = vec_grid(n), Gp = precond_grid();
   const PcView view{pc ? pc->q_basis : nullptr, pc ? pc->w_core : nullptr, n, nr,
                     pc ? pc->ldq : 4, pc ? pc->inv_sqrt_iso : 1.0};
@@ -441,7 +441,7 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
     for (int c = 0; c < chunk; ++c) {
       t32.begin(s);
       if (sym) {
-        launch_k1s(op->packed32, n, d, op->clamp, w.p, w.part32, sym_col, sp, dstatus,
+        launch_k1s(op->packed32, n, d, op->clamp, w.p, sym_row, sym_col, sp, dstatus,
                    &w.st->active, s);
       } else {
         launch_k1(op->packed32, n, op->packed32, n, d, op->clamp, w.p, w.part32, p1, dstatus,
@@ -449,10 +449,10 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
       }
       t32.end(s);
       if (sym)
-        pcg_after_matvec_kernel<true><<<G, T, 0, s>>>(w.part32, 0, sp, sym_col, w.p, w.Ap, n,
+        pcg_after_matvec_kernel<true><<<G, T, 0, s>>>(w.part32, 0, sp, sym_row, sym_col, w.p, w.Ap, n,
                                                       w.blockpart, w.st);
       else
-        pcg_after_matvec_kernel<false><<<G, T, 0, s>>>(w.part32, p1.S, sp, nullptr, w.p, w.Ap, n,
+        pcg_after_matvec_kernel<false><<<G, T, 0, s>>>(w.part32, p1.S, sp, nullptr, nullptr, w.p, w.Ap, n,
                                                        w.blockpart, w.st);
       pcg_update_xr_kernel<<<G, T, 0, s>>>(w.p, w.Ap, X, w.r, n, w.blockpart, w.st);
       t64.begin(s);

@@ -11,15 +11,32 @@ namespace laker {
 // Blocks of B points; pairs (a, b), a <= b, row-major over the upper triangle;
 // CTA c owns pairs [c*q + min(c, rem), ... + q + (c < rem)).
 struct SymPlan {
-  int64_t nb;      // number of point blocks
-  int64_t npairs;  // nb (nb + 1) / 2
+  int64_t nb;      // number of point blocks (all instances)
+  int64_t npairs;  // number of block pairs (all instances)
   int64_t q, rem;  // pairs per CTA
   int grid;        // CTAs
   int B;           // points per block
   int cfg;         // kernel variant
 };
 
-// Index of pair (a, b), a <= b.
+// Several independent problems in one launch: instance k owns the global
+// points [seg[k], seg[k] + npts[k]) (seg a multiple of 256, so its packed
+// embeddings start on a column tile), nblk[k] blocks and the global pairs
+// [pair_start[k], pair_start[k+1]); its blocks are global blocks
+// blk_start[k] .. blk_start[k+1]-1.  Pairs only pair blocks of the same
+// instance, so the operator is block diagonal.  done[k] != 0 skips an
+// instance (converged).  All arrays are device memory.
+struct BatchMap {
+  int count;
+  const int64_t* pair_start;  // [count + 1]
+  const int64_t* nblk;        // [count]
+  const int64_t* npts;        // [count]
+  const int64_t* seg;         // [count]
+  const int64_t* blk_start;   // [count + 1]
+  const int* done;            // [count] or null
+};
+
+// Index of pair (a, b), a <= b, among the nb (nb + 1) / 2 pairs of nb blocks.
 __host__ __device__ inline int64_t sym_pair_index(int64_t a, int64_t b, int64_t nb) {
   return a * nb - a * (a - 1) / 2 + (b - a);
 }
@@ -41,37 +58,51 @@ __host__ __device__ inline void sym_pair_coords(int64_t p, int64_t nb, int64_t* 
   *b = r + (p - sym_first_pair(r, nb));
 }
 
-// CTA that owns pair p.
-__host__ __device__ inline int64_t sym_cta_of(int64_t p, const SymPlan& sp) {
-  const int64_t big = sp.rem * (sp.q + 1);
-  if (p < big) return p / (sp.q + 1);
-  return sp.q > 0 ? sp.rem + (p - big) / sp.q : sp.rem;
-}
-
-// sum_j K_ij x_j for row i from the partials of one symmetric matvec:
-// the row-sum runs of the CTAs that processed row block a = i / B (slot
-// cta + a), then the column sums of the pairs (a', a), a' < a, in order.
-__device__ inline double sym_row_sum(const SymPlan& sp, const double* __restrict__ rowpart,
-                                     const float* __restrict__ colpart, int64_t i) {
-  const int64_t a = i / sp.B, o = i - a * sp.B;
-  const int64_t c0 = sym_cta_of(sym_first_pair(a, sp.nb), sp);
-  const int64_t c1 = sym_cta_of(sym_first_pair(a, sp.nb) + (sp.nb - a) - 1, sp);
+// sum_j K_ij x_j for local row li of an instance whose pairs start at global
+// pair ps: the row sums of its pairs (a, b >= a), then the column sums of its
+// pairs (a' < a, a), in that fixed order.  Both partial arrays hold one
+// B-vector per pair.
+__device__ inline double sym_instance_row_sum(int64_t nb, int64_t ps, int B,
+                                              const float* __restrict__ rowpart,
+                                              const float* __restrict__ colpart, int64_t li) {
+  const int64_t a = li / B, o = li - a * B;
+  const int64_t f = ps + sym_first_pair(a, nb);
   double s = 0.0;
-  for (int64_t c = c0; c <= c1; ++c) s += rowpart[(c + a) * sp.B + o];
-  for (int64_t ap = 0; ap < a; ++ap) s += (double)colpart[sym_pair_index(ap, a, sp.nb) * sp.B + o];
+  for (int64_t q = 0; q < nb - a; ++q) s += (double)rowpart[(f + q) * B + o];
+  for (int64_t ap = 0; ap < a; ++ap) s += (double)colpart[(ps + sym_pair_index(ap, a, nb)) * B + o];
   return s;
 }
 
+// Single instance.
+__device__ inline double sym_row_sum(const SymPlan& sp, const float* __restrict__ rowpart,
+                                     const float* __restrict__ colpart, int64_t i) {
+  return sym_instance_row_sum(sp.nb, 0, sp.B, rowpart, colpart, i);
+}
+
+// Batched layout: local row li of instance k.
+__device__ inline double sym_row_sum_batched(const SymPlan& sp, const BatchMap& bm,
+                                             const float* __restrict__ rowpart,
+                                             const float* __restrict__ colpart, int k, int64_t li) {
+  return sym_instance_row_sum(bm.nblk[k], bm.pair_start[k], sp.B, rowpart, colpart, li);
+}
+
+// Points per block of the symmetric kernel.
+int sym_block_points();
 // Plan for n points of padded dimension from d.
 SymPlan k1s_plan(int64_t n, int d);
-// Workspace pieces: rowpart (grid + nb) x B doubles, colpart npairs x B floats.
-inline size_t sym_rowpart_elems(const SymPlan& sp) { return (size_t)(sp.grid + sp.nb) * sp.B; }
+// Plan for an explicit pair list (batched layout: nb = total blocks).
+SymPlan k1s_plan_pairs(int64_t nb, int64_t npairs, int d);
+// Workspace pieces: row and column partials, one B-vector of floats per pair.
+inline size_t sym_rowpart_elems(const SymPlan& sp) { return (size_t)sp.npairs * sp.B; }
 inline size_t sym_colpart_elems(const SymPlan& sp) { return (size_t)sp.npairs * sp.B; }
 cudaError_t launch_k1s(const float* E32, int64_t n, int d, int clamp, const float* x,
-                       double* rowpart, float* colpart, const SymPlan& sp, int* status,
+                       float* rowpart, float* colpart, const SymPlan& sp, int* status,
                        const int* gate, cudaStream_t s);
+cudaError_t launch_k1s_batched(const float* E32, int d, int clamp, const float* x,
+                               float* rowpart, float* colpart, const SymPlan& sp,
+                               const BatchMap& bm, int* status, const int* gate, cudaStream_t s);
 // y = lam x + (sum of the partials) for the standalone matvec.
-cudaError_t launch_sym_finish(const SymPlan& sp, const double* rowpart, const float* colpart,
+cudaError_t launch_sym_finish(const SymPlan& sp, const float* rowpart, const float* colpart,
                               int64_t n, float lam, const float* x, float* y, int64_t ldy,
                               cudaStream_t s);
 // Whether square FP32 matvecs use the symmetric kernel (LAKER_K1_SYMMETRIC=0
@@ -79,8 +110,12 @@ cudaError_t launch_sym_finish(const SymPlan& sp, const double* rowpart, const fl
 bool k1_use_symmetric();
 // Bytes of the symmetric partials (rowpart, then colpart at a 256-byte boundary).
 inline size_t sym_partial_bytes(const SymPlan& sp) {
-  return (size_t)round_up((int64_t)(sym_rowpart_elems(sp) * sizeof(double)), 256) +
+  return (size_t)round_up((int64_t)(sym_rowpart_elems(sp) * sizeof(float)), 256) +
          sym_colpart_elems(sp) * sizeof(float);
+}
+inline float* sym_colpart_ptr(void* partials, const SymPlan& sp) {
+  return reinterpret_cast<float*>(static_cast<char*>(partials) +
+                                  round_up((int64_t)(sym_rowpart_elems(sp) * sizeof(float)), 256));
 }
 
 }  // namespace laker

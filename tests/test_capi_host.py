@@ -60,6 +60,18 @@ def test_workspace_and_layout_queries():
     assert lib.laker_pcg_workspace_bytes(100000, 10, 256, 1) > 100000 * 8
     assert lib.laker_pcg_workspace_bytes(0, 10, 256, 1) == 0
     assert lib.laker_precond_workspace_bytes(1000, 2000, 1) == 0  # nr > 1024
+    # batched layout: instances at 256-point aligned offsets
+    ns = (ctypes.c_int64 * 3)(1, 256, 257)
+    offs = (ctypes.c_int64 * 4)()
+    assert lib.laker_batch_layout(3, ns, offs) == 1024
+    assert list(offs) == [0, 256, 512, 1024]
+    assert lib.laker_pcg_batched_workspace_bytes(3, ns, 6) > 1024 * 8
+    assert lib.laker_pcg_batched_workspace_bytes(3, ns, 17) == 0
+    assert lib.laker_pcg_batched_workspace_bytes(0, ns, 6) == 0
+    res = (_lib.laker_pcg_result * 3)()
+    prm = _lib.laker_pcg_params(1e-6, 10, 0.1, 1e-8, 1, 0, 0)
+    assert lib.laker_pcg_solve_batched(None, None, None, ctypes.byref(prm), None, 0, res,
+                                       None) == _lib.LAKER_ERR_INVALID_ARG
 
 
 def test_estimator_validation_messages():
