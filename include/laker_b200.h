@@ -250,16 +250,22 @@ typedef struct laker_batch {
   const laker_precond* precond; /* HOST [count] (device factors) or NULL       */
 } laker_batch;
 
-size_t laker_pcg_batched_workspace_bytes(int count, const int64_t* n, int d);
+/* Workspace for a batch whose preconditioners have at most max_nr probes
+ * (0: no preconditioner); 0 for invalid sizes. */
+size_t laker_pcg_batched_workspace_bytes(int count, const int64_t* n, int d, int max_nr);
 
 /* Solves A_k x_k = b_k for every instance with the mixed-precision PCG of
- * laker_pcg_solve in one device loop: one symmetric FP32 matvec launch covers
- * all unconverged instances (block-diagonal pair list), every other step runs
- * one CTA per instance, per-instance scalars and convergence masks live on the
- * device, and the iteration is captured once as a CUDA graph and replayed
- * until every instance has stopped.  B, X: batched vectors (padded length).
- * results: HOST array of count results.  Returns LAKER_OK unless a call
- * failed; per-instance outcomes are in results[k].status.
+ * laker_pcg_solve in one device loop.  Per iteration: one symmetric FP32
+ * matvec launch over the block pairs of the instances still running (the list
+ * is compacted on the device after every iteration, so the whole grid works on
+ * what is left), then vector kernels with one CTA per 512-point block of every
+ * running instance and per-instance reductions in a fixed order; scalars and
+ * convergence masks live on the device and the iteration is captured once as a
+ * CUDA graph and replayed until every instance has stopped.  An instance's
+ * result does not depend on the other instances of the batch.  B, X: batched
+ * vectors (padded length).  results: HOST array of count results.  Returns
+ * LAKER_OK unless a call failed; per-instance outcomes are in
+ * results[k].status.  Warm starts (has_x0) are not supported.
  * Replaces a loop of PreconditionedConjugateGradient.solve calls
  * (laker/solvers.py:130-295) over independent problems. */
 int laker_pcg_solve_batched(const laker_batch* batch, const double* B, double* X,

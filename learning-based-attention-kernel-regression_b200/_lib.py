@@ -109,7 +109,7 @@ class laker_batch(ctypes.Structure):
 _P = c_void_p
 _SIGNATURES = {
     "laker_batch_layout": (c_int64, [c_int, POINTER(c_int64), POINTER(c_int64)]),
-    "laker_pcg_batched_workspace_bytes": (c_size_t, [c_int, POINTER(c_int64), c_int]),
+    "laker_pcg_batched_workspace_bytes": (c_size_t, [c_int, POINTER(c_int64), c_int, c_int]),
     "laker_pcg_solve_batched": (
         c_int,
         [POINTER(laker_batch), _P, _P, POINTER(laker_pcg_params), _P, c_size_t,

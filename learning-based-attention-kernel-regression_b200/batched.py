@@ -9,9 +9,10 @@ a per-instance convergence mask that freezes each instance at the iteration the
 reference would stop at -- and a final per-instance eigh for the apply.
 
 `BatchedPCG.solve` runs laker_pcg_solve_batched: one device loop for all
-instances (block-diagonal symmetric FP32 matvec over all unconverged
-instances, one CTA per instance for every vector step, per-instance scalars and
-convergence masks on the device, the iteration replayed as a CUDA graph).
+instances (block-diagonal symmetric FP32 matvec over the block pairs of the
+instances still running, vector steps over 512-point blocks with per-instance
+reductions in a fixed order, per-instance scalars and convergence masks on the
+device, the iteration replayed as a CUDA graph).
 """
 
 from __future__ import annotations
@@ -192,7 +193,8 @@ class BatchedPCG:
         params = _lib.laker_pcg_params(self.tol, self.max_iter, self.reliable_delta,
                                        torch.finfo(torch.float32).eps ** 0.5, self.check_every,
                                        0, 0)
-        ws = _lib.workspace(lib.laker_pcg_batched_workspace_bytes(count, ns, d), dev)
+        max_nr = max(p.nr for p in preconditioners) if preconditioners is not None else 0
+        ws = _lib.workspace(lib.laker_pcg_batched_workspace_bytes(count, ns, d, max_nr), dev)
         results = (_lib.laker_pcg_result * count)()
         _lib.check(lib.laker_pcg_solve_batched(ctypes.byref(batch), b.data_ptr(), x.data_ptr(),
                                                ctypes.byref(params), ws.data_ptr(), ws.numel(),

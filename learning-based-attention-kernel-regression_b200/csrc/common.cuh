@@ -136,6 +136,31 @@ __device__ __forceinline__ V warp_sum(V v) {
   return v;
 }
 
+// Warp sums of V values per lane (V a power of two, 2..32) by recursive
+// halving: at each of the first log2 V butterfly steps a lane keeps half of
+// its values and sends the other half to its partner, so the step count and
+// the additions fall from 5 V to V - 1 + 5 - log2 V.  On return v[0] of lane l
+// holds the warp sum of value index l >> (5 - log2 V) (the same sum in the
+// 32 / V lanes that share those bits).  Fixed order: deterministic.
+template <int V, typename F>
+__device__ __forceinline__ F warp_reduce_scatter(F (&v)[V], int lane) {
+  static_assert(V >= 2 && V <= 32 && (V & (V - 1)) == 0, "V must be a power of two in [2, 32]");
+  int o = 16;
+#pragma unroll
+  for (int h = V / 2; h >= 1; h >>= 1, o >>= 1) {
+    const bool up = (lane & o) != 0;
+#pragma unroll
+    for (int i = 0; i < h; ++i) {
+      const F keep = up ? v[i + h] : v[i];
+      const F send = up ? v[i] : v[i + h];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+    }
+  }
+#pragma unroll
+  for (; o > 0; o >>= 1) v[0] += __shfl_xor_sync(0xffffffffu, v[0], o);
+  return v[0];
+}
+
 // Sums NV values over the block; result valid in every thread of warp 0.
 // `scratch` must hold NV * (T/32) doubles.
 template <int T, int NV>
@@ -158,15 +183,15 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* scratch) {
   __syncthreads();
 }
 
-// Grid completion detector for "last block finishes the reduction": every
-// block publishes its partials, then calls this; exactly one block (the last
-// to arrive) gets true.  The counter is reset by that block for reuse.
-__device__ __forceinline__ bool arrive_last_block(unsigned int* counter) {
+// Completion detector for "last block finishes the reduction": each of
+// `total` blocks publishes its partials, then calls this; exactly one block
+// (the last to arrive) gets true.  The counter is reset by that block for
+// reuse.
+__device__ __forceinline__ bool arrive_last_of(unsigned int* counter, unsigned int total) {
   __shared__ bool s_last;
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
-    const unsigned int total = gridDim.x * gridDim.y * gridDim.z;
     const unsigned int t = atomicAdd(counter, 1u);
     s_last = (t == total - 1);
     if (s_last) *counter = 0;  // every block has arrived; safe to rearm
@@ -174,6 +199,11 @@ __device__ __forceinline__ bool arrive_last_block(unsigned int* counter) {
   __syncthreads();
   if (s_last) __threadfence();
   return s_last;
+}
+
+// Same over the whole grid.
+__device__ __forceinline__ bool arrive_last_block(unsigned int* counter) {
+  return arrive_last_of(counter, gridDim.x * gridDim.y * gridDim.z);
 }
 
 }  // namespace laker

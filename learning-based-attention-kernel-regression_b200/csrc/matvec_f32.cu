@@ -451,9 +451,10 @@ extern "C" size_t laker_matvec_workspace_bytes(int64_t m, int64_t n, int d, int 
   if (k > 1) return kWsHeader;
   const SegPlan p = precision == 64 ? k4_plan(m, n, d) : k1_plan(m, n, d);
   size_t bytes = (size_t)p.S * (size_t)m * sizeof(double);
-  if (precision != 64 && m == n && n > 0) {
+  if (m == n && n > 0) {
     // a square product with the same embeddings may take the symmetric kernel
-    const size_t sym = sym_partial_bytes(k1s_plan(n, d));
+    const size_t sym = precision == 64 ? sym_partial_bytes<double>(k4s_plan(n, d))
+                                       : sym_partial_bytes<float>(k1s_plan(n, d));
     if (sym > bytes) bytes = sym;
   }
   return kWsHeader + bytes;
@@ -482,8 +483,8 @@ extern "C" int laker_attn_matvec_f32(const float* rows32, int64_t m, const float
   if (rows32 == cols32 && m == n && k1_use_symmetric()) {
     // the operator itself: every off-diagonal entry evaluated once
     const SymPlan sp = k1s_plan(n, d);
-    float* rowpart = reinterpret_cast<float*>(wbase);
-    float* colpart = sym_colpart_ptr(wbase, sp);
+    double* rowpart = reinterpret_cast<double*>(wbase);
+    float* colpart = sym_colpart_ptr<float>(wbase, sp);
     e = launch_k1s(cols32, n, d, clamp, X, rowpart, colpart, sp, &hdr->status, nullptr, s);
     if (e == cudaSuccess) e = launch_sym_finish(sp, rowpart, colpart, n, lam, X, Y, ldy, s);
     return e == cudaSuccess ? LAKER_OK : fail_cuda(e);

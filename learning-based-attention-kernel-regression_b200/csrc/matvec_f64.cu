@@ -6,7 +6,7 @@
 // so the result carries the float64 reference operator's accuracy: the PCG
 // loop uses it to recompute the true residual b - A x, and float64 operators
 // and predictions use it directly.
-#include "internal.cuh"
+#include "sym.cuh"
 
 namespace laker {
 namespace {
@@ -214,8 +214,18 @@ extern "C" int laker_attn_matvec_f64(const double* rows64, int64_t m, const doub
                          Y, ldy, s);
     return e == cudaSuccess ? LAKER_OK : fail_cuda(e);
   }
+  char* wbase = static_cast<char*>(workspace) + kWsHeader;
+  if (rows64 == cols64 && m == n && ldx == 1 && k4_use_symmetric()) {
+    // the operator itself: every off-diagonal entry evaluated once
+    const SymPlan sp = k4s_plan(n, d);
+    double* rowpart = reinterpret_cast<double*>(wbase);
+    double* colpart = sym_colpart_ptr<double>(wbase, sp);
+    e = launch_k4s(rows64, n, d, clamp, X, rowpart, colpart, sp, &hdr->status, nullptr, s);
+    if (e == cudaSuccess) e = launch_sym_finish64(sp, rowpart, colpart, n, lam, X, B, ldb, Y, ldy, s);
+    return e == cudaSuccess ? LAKER_OK : fail_cuda(e);
+  }
   const SegPlan plan = k4_plan(m, n, d);
-  double* part = reinterpret_cast<double*>(static_cast<char*>(workspace) + kWsHeader);
+  double* part = reinterpret_cast<double*>(wbase);
   if (n > 0) {
     if (ldx != 1) return LAKER_ERR_UNSUPPORTED;
     e = launch_k4(rows64, m, cols64, n, d, clamp, X, part, plan, &hdr->status, nullptr, s);

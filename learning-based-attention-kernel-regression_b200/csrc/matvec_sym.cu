@@ -18,8 +18,9 @@
 // i.e. (d + 2) / 2 FMA and 1/2 exp2 per logical entry.
 //
 // The BATCHED instantiation runs many independent problems in one launch
-// (BatchMap): the pair list is the concatenation of the instances' pair
-// lists, so the operator is block diagonal; converged instances are skipped.
+// (BatchMap): the pair list is the concatenation of the running instances'
+// pair lists (a block-diagonal operator), split evenly over the grid at run
+// time, so the whole grid works on whatever is still running.
 #include <cstdlib>
 
 #include "sym.cuh"
@@ -27,26 +28,30 @@
 namespace laker {
 namespace {
 
-// Position in a CTA's flat sequence of column tiles (pair p, tile t of block b).
+// Position in a CTA's flat sequence of column tiles (pair p, tile t of block
+// b).  p counts the pairs of the launch; the pair's partial sums live at slot
+// gp0 + (p - pstart).
 struct SymCursor {
   int64_t p, p_end;
-  int inst;
+  int j;  // index into the running-instance list (batched)
   int64_t a, b;
   int t;
-  // metadata of instance `inst`
-  int64_t nb, npts, seg, blk0, pstart, pend;
+  // metadata of the current instance
+  int64_t nb, npts, seg, blk0, pstart, pend, gp0;
 };
 
 template <bool BATCHED>
 __device__ __forceinline__ void cursor_load_inst(SymCursor& cu, const SymPlan& sp,
                                                  const BatchMap& bm, int64_t n) {
   if (BATCHED) {
-    cu.nb = bm.nblk[cu.inst];
-    cu.npts = bm.npts[cu.inst];
-    cu.seg = bm.seg[cu.inst];
-    cu.blk0 = bm.blk_start[cu.inst];
-    cu.pstart = bm.pair_start[cu.inst];
-    cu.pend = bm.pair_start[cu.inst + 1];
+    const int k = bm.act_inst[cu.j];
+    cu.nb = bm.nblk[k];
+    cu.npts = bm.npts[k];
+    cu.seg = bm.seg[k];
+    cu.blk0 = bm.blk_start[k];
+    cu.pstart = bm.act_ps[cu.j];
+    cu.pend = bm.act_ps[cu.j + 1];
+    cu.gp0 = bm.pair_start[k];
   } else {
     cu.nb = sp.nb;
     cu.npts = n;
@@ -54,30 +59,25 @@ __device__ __forceinline__ void cursor_load_inst(SymCursor& cu, const SymPlan& s
     cu.blk0 = 0;
     cu.pstart = 0;
     cu.pend = sp.npairs;
+    cu.gp0 = 0;
   }
 }
 
-// Place the cursor on tile 0 of pair p, moving past finished instances.
+// Place the cursor on tile 0 of pair p, moving to the instance that holds it.
 // Returns false when the CTA's range is exhausted.
 template <bool BATCHED>
 __device__ __forceinline__ bool cursor_settle(SymCursor& cu, const SymPlan& sp, const BatchMap& bm,
                                               int64_t n) {
-  for (;;) {
-    if (cu.p >= cu.p_end) return false;
-    if (BATCHED) {
-      while (cu.p >= cu.pend) {
-        ++cu.inst;
-        cursor_load_inst<BATCHED>(cu, sp, bm, n);
-      }
-      if (bm.done && bm.done[cu.inst]) {
-        cu.p = cu.pend;
-        continue;
-      }
+  if (cu.p >= cu.p_end) return false;
+  if (BATCHED) {
+    while (cu.p >= cu.pend) {  // ends: p < p_end <= act_ps[*act_count]
+      ++cu.j;
+      cursor_load_inst<BATCHED>(cu, sp, bm, n);
     }
-    sym_pair_coords(cu.p - cu.pstart, cu.nb, &cu.a, &cu.b);
-    cu.t = 0;
-    return true;
   }
+  sym_pair_coords(cu.p - cu.pstart, cu.nb, &cu.a, &cu.b);
+  cu.t = 0;
+  return true;
 }
 
 // Next tile that holds points (tiles starting at or past the instance's n are
@@ -103,7 +103,7 @@ __device__ __forceinline__ bool cursor_next(SymCursor& cu, const SymPlan& sp, co
 template <int DP, int R, int T, bool CLAMP, bool BATCHED>
 __global__ void __launch_bounds__(T, 3)
     k1s_matvec_f32(const float* __restrict__ E, int64_t n, const float* __restrict__ x,
-                   float* __restrict__ colpart, float* __restrict__ rowpart, SymPlan sp,
+                   float* __restrict__ colpart, double* __restrict__ rowpart, SymPlan sp,
                    BatchMap bm, int* status, const int* gate) {
   if (gate && *gate == 0) return;
   constexpr int TC = kTileCols32;
@@ -120,24 +120,32 @@ __global__ void __launch_bounds__(T, 3)
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t c = blockIdx.x;
-  const int64_t p_begin = c * sp.q + (c < sp.rem ? c : sp.rem);
-  const int64_t p_end = p_begin + sp.q + (c < sp.rem ? 1 : 0);
-  if (p_begin >= p_end) return;
-
-  // consumer cursor (cu) and prefetch cursor (nx) over the same tile sequence
+  int64_t p_begin, p_end;
   SymCursor cu;
-  cu.p = p_begin;
-  cu.p_end = p_end;
-  cu.inst = 0;
+  cu.j = 0;
   if (BATCHED) {
-    // instance of the first pair: binary search of pair_start
-    int lo = 0, hi = bm.count - 1;
+    // split the running instances' pairs evenly over the grid
+    const int nact = *bm.act_count;
+    if (nact <= 0) return;
+    const int64_t total = bm.act_ps[nact];
+    const int64_t q = total / gridDim.x, rem = total % gridDim.x;
+    p_begin = c * q + (c < rem ? c : rem);
+    p_end = p_begin + q + (c < rem ? 1 : 0);
+    if (p_begin >= p_end) return;
+    // running instance of the first pair: binary search of act_ps
+    int lo = 0, hi = nact - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
-      if (bm.pair_start[mid] <= p_begin) lo = mid; else hi = mid - 1;
+      if (bm.act_ps[mid] <= p_begin) lo = mid; else hi = mid - 1;
     }
-    cu.inst = lo;
+    cu.j = lo;
+  } else {
+    p_begin = c * sp.q + (c < sp.rem ? c : sp.rem);
+    p_end = p_begin + sp.q + (c < sp.rem ? 1 : 0);
+    if (p_begin >= p_end) return;
   }
+  cu.p = p_begin;
+  cu.p_end = p_end;
   cursor_load_inst<BATCHED>(cu, sp, bm, n);
   if (!cursor_settle<BATCHED>(cu, sp, bm, n)) return;  // uniform: every thread sees the same
 
@@ -158,7 +166,7 @@ __global__ void __launch_bounds__(T, 3)
     for (int j = tid; j < TC; j += T) sX[buf][j] = (local0 + j < s.npts) ? x[s.seg + local0 + j] : 0.0f;
   };
 
-  // rows of block (cu.inst, cu.a) in registers; row sums of the current pair
+  // rows of block a of the current instance in registers; row sums of the current pair
   float2 ev[R][DP];
   float2 xr[R];
   double acc[R];
@@ -184,10 +192,10 @@ __global__ void __launch_bounds__(T, 3)
   // a fixed order that does not depend on which CTA processed them (the
   // result is the same alone or inside any batch).
   auto flush_rows = [&](int64_t pair) {
-    float* dst = rowpart + pair * (int64_t)B;
+    double* dst = rowpart + pair * (int64_t)B;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      dst[r * T + tid] = (float)acc[r];
+      dst[r * T + tid] = acc[r];
       acc[r] = 0.0;
     }
   };
@@ -257,23 +265,16 @@ __global__ void __launch_bounds__(T, 3)
           }
           cs[u] = ca;
         }
-        // warp reduction of the 16 column partials (fixed butterfly order)
+        // warp sums of the 16 column partials (columns 2 q0 .. 2 q0 + 15):
+        // reduce-scatter, lane l ends with column 2 q0 + (l >> 1)
+        float cv16[16];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            cs[u].x += __shfl_xor_sync(0xffffffffu, cs[u].x, o);
-            cs[u].y += __shfl_xor_sync(0xffffffffu, cs[u].y, o);
-          }
+        for (int u = 0; u < 8; ++u) {
+          cv16[2 * u] = cs[u].x;
+          cv16[2 * u + 1] = cs[u].y;
         }
-        if (lane < 8) {
-          // lane u stores column pair q0 + u (a register select per lane)
-          float2 mine = cs[0];
-#pragma unroll
-          for (int u = 1; u < 8; ++u)
-            if (lane == u) mine = cs[u];
-          reinterpret_cast<float2*>(sCol[warp])[q0 + lane] = mine;
-        }
+        const float colsum = warp_reduce_scatter<16>(cv16, lane);
+        if ((lane & 1) == 0) sCol[warp][2 * q0 + (lane >> 1)] = colsum;
       }
     } else {
 #pragma unroll 2
@@ -312,17 +313,196 @@ __global__ void __launch_bounds__(T, 3)
         float s = 0.0f;
 #pragma unroll
         for (int w = 0; w < NW; ++w) s += sCol[w][j];
-        colpart[cu.p * (int64_t)B + cu.t * TC + j] = s;
+        colpart[(cu.gp0 + cu.p - cu.pstart) * B + cu.t * TC + j] = s;
       }
     }
     __syncthreads();  // sCol is reused by the next tile
 
     // advance the consumer; store the row sums when the pair changes and
     // reload the rows when the row block changes
-    const int64_t prev_pair = cu.p, prev_block = cu.blk0 + cu.a;
+    const int64_t prev_p = cu.p, prev_slot = cu.gp0 + cu.p - cu.pstart;
+    const int64_t prev_block = cu.blk0 + cu.a;
     const bool more = cursor_next<BATCHED, B, TC, TPB>(cu, sp, bm, n);
     ++k_tile;
-    if (!more || cu.p != prev_pair) flush_rows(prev_pair);
+    if (!more || cu.p != prev_p) flush_rows(prev_slot);
+    if (more && cu.blk0 + cu.a != prev_block) load_rows(cu);
+    if (!more) break;
+    if (have_nx) have_nx = cursor_next<BATCHED, B, TC, TPB>(nx, sp, bm, n);
+  }
+  if (failed) {
+    for (int k = consumed + 1; k < issued; ++k) mbar_wait_bounded(&bar[k & 1], (k >> 1) & 1, status);
+  }
+}
+
+// FP64 twin of k1s_matvec_f32 (the accurate operator of the residual
+// recomputation): the same blocks, pairs, cursors and per-pair partial sums,
+// with FP64 logits, exp and accumulation.  Column tiles are packed64 rows
+// (TC points of DP doubles, one TMA bulk copy each); R rows per thread.
+template <int DP, int R, int T, bool CLAMP, bool BATCHED>
+__global__ void __launch_bounds__(T, 1)
+    k4s_matvec_f64(const double* __restrict__ E, int64_t n, const double* __restrict__ x,
+                   double* __restrict__ colpart, double* __restrict__ rowpart, SymPlan sp,
+                   BatchMap bm, int* status, const int* gate) {
+  if (gate && *gate == 0) return;
+  constexpr int TC = kTileCols64;
+  constexpr int TILE = TC * DP;
+  constexpr int B = T * R;
+  constexpr int TPB = B / TC;
+  constexpr int NW = T / 32;
+  constexpr int CB = 8;  // columns whose partials are reduced together
+  static_assert(B % TC == 0, "block must be a whole number of column tiles");
+  __shared__ __align__(128) double sE[2][TILE];
+  __shared__ __align__(16) double sX[2][TC];
+  __shared__ double sCol[NW][TC];
+  __shared__ __align__(8) uint64_t bar[2];
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t c = blockIdx.x;
+  int64_t p_begin, p_end;
+  SymCursor cu;
+  cu.j = 0;
+  if (BATCHED) {
+    const int nact = *bm.act_count;
+    if (nact <= 0) return;
+    const int64_t total = bm.act_ps[nact];
+    const int64_t q = total / gridDim.x, rem = total % gridDim.x;
+    p_begin = c * q + (c < rem ? c : rem);
+    p_end = p_begin + q + (c < rem ? 1 : 0);
+    if (p_begin >= p_end) return;
+    int lo = 0, hi = nact - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (bm.act_ps[mid] <= p_begin) lo = mid; else hi = mid - 1;
+    }
+    cu.j = lo;
+  } else {
+    p_begin = c * sp.q + (c < sp.rem ? c : sp.rem);
+    p_end = p_begin + sp.q + (c < sp.rem ? 1 : 0);
+    if (p_begin >= p_end) return;
+  }
+  cu.p = p_begin;
+  cu.p_end = p_end;
+  cursor_load_inst<BATCHED>(cu, sp, bm, n);
+  if (!cursor_settle<BATCHED>(cu, sp, bm, n)) return;
+
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+
+  auto col0_of = [&](const SymCursor& s) -> int64_t { return s.seg + s.b * B + (int64_t)s.t * TC; };
+  auto issue = [&](int64_t col0, int buf) {
+    mbar_arrive_expect_tx(&bar[buf], TILE * 8);
+    bulk_g2s(sE[buf], E + col0 * DP, TILE * 8, &bar[buf]);
+  };
+  auto load_x = [&](const SymCursor& s, int buf) {
+    const int64_t local0 = s.b * B + (int64_t)s.t * TC;
+    for (int j = tid; j < TC; j += T) sX[buf][j] = (local0 + j < s.npts) ? x[s.seg + local0 + j] : 0.0;
+  };
+
+  double ev[R][DP], xr[R], acc[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) acc[r] = 0.0;
+  auto load_rows = [&](const SymCursor& s) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int64_t li = s.a * B + r * T + tid;
+      const bool ok = li < s.npts;
+      const int64_t i = s.seg + li;
+#pragma unroll
+      for (int k = 0; k < DP; ++k) ev[r][k] = ok ? E[i * DP + k] : 0.0;
+      xr[r] = ok ? x[i] : 0.0;
+    }
+  };
+  auto flush_rows = [&](int64_t slot) {
+    double* dst = rowpart + slot * (int64_t)B;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      dst[r * T + tid] = acc[r];
+      acc[r] = 0.0;
+    }
+  };
+  auto entry = [&](const double* cp, int r) -> double {
+    double s = ev[r][0] * cp[0];
+#pragma unroll
+    for (int k = 1; k < DP; ++k) s = fma(ev[r][k], cp[k], s);
+    if (CLAMP) s = fmin(s, kClamp64);
+    return exp(s);
+  };
+
+  load_rows(cu);
+  SymCursor nx = cu;
+  if (tid == 0) issue(col0_of(nx), 0);
+  load_x(nx, 0);
+  bool have_nx = cursor_next<BATCHED, B, TC, TPB>(nx, sp, bm, n);
+  __syncthreads();
+
+  int k_tile = 0, issued = 1, consumed = 0;
+  bool failed = false;
+  for (;;) {
+    const int buf = k_tile & 1;
+    if (have_nx) {
+      if (tid == 0) issue(col0_of(nx), buf ^ 1);
+      load_x(nx, buf ^ 1);
+      ++issued;
+    }
+    const int ok = __syncthreads_and(mbar_wait_bounded(&bar[buf], (k_tile >> 1) & 1, status) ? 1 : 0);
+    if (!ok) {
+      failed = true;
+      break;
+    }
+    ++consumed;
+    const bool offdiag = cu.a != cu.b;
+    const double* Et = sE[buf];
+    const double* Xt = sX[buf];
+    if (offdiag) {
+#pragma unroll 1
+      for (int j0 = 0; j0 < TC; j0 += CB) {
+        double cs[CB];
+#pragma unroll
+        for (int u = 0; u < CB; ++u) {
+          const double* cp = Et + (j0 + u) * DP;
+          const double xj = Xt[j0 + u];
+          double ca = 0.0;
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const double e = entry(cp, r);
+            acc[r] = fma(e, xj, acc[r]);
+            ca = fma(e, xr[r], ca);
+          }
+          cs[u] = ca;
+        }
+        // reduce-scatter: lane l ends with column j0 + l / (32 / CB)
+        const double colsum = warp_reduce_scatter<CB>(cs, lane);
+        if ((lane & (32 / CB - 1)) == 0) sCol[warp][j0 + lane / (32 / CB)] = colsum;
+      }
+    } else {
+#pragma unroll 2
+      for (int j = 0; j < TC; ++j) {
+        const double* cp = Et + j * DP;
+        const double xj = Xt[j];
+#pragma unroll
+        for (int r = 0; r < R; ++r) acc[r] = fma(entry(cp, r), xj, acc[r]);
+      }
+    }
+    __syncthreads();  // sE/sX[buf] are refilled next; sCol is complete
+    if (offdiag) {
+      for (int j = tid; j < TC; j += T) {
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) s += sCol[w][j];
+        colpart[(cu.gp0 + cu.p - cu.pstart) * B + cu.t * TC + j] = s;
+      }
+    }
+    __syncthreads();
+
+    const int64_t prev_p = cu.p, prev_slot = cu.gp0 + cu.p - cu.pstart;
+    const int64_t prev_block = cu.blk0 + cu.a;
+    const bool more = cursor_next<BATCHED, B, TC, TPB>(cu, sp, bm, n);
+    ++k_tile;
+    if (!more || cu.p != prev_p) flush_rows(prev_slot);
     if (more && cu.blk0 + cu.a != prev_block) load_rows(cu);
     if (!more) break;
     if (have_nx) have_nx = cursor_next<BATCHED, B, TC, TPB>(nx, sp, bm, n);
@@ -342,7 +522,7 @@ constexpr int kSymRows = 4;      // rows per thread
 constexpr int kSymThreads = 128;  // threads per CTA -> B = 512 points per block
 
 template <int DP, bool CLAMP, bool BATCHED>
-cudaError_t launch_k1s_t(const float* E, int64_t n, const float* x, float* rowpart,
+cudaError_t launch_k1s_t(const float* E, int64_t n, const float* x, double* rowpart,
                          float* colpart, const SymPlan& sp, const BatchMap& bm, int* status,
                          const int* gate, cudaStream_t s) {
   k1s_matvec_f32<DP, kSymRows, kSymThreads, CLAMP, BATCHED>
@@ -385,12 +565,60 @@ int k1s_occupancy(int dp) {
     default: return cudaErrorInvalidValue;              \
   }
 
-__global__ void sym_finish_kernel(SymPlan sp, const float* __restrict__ rowpart,
+constexpr int kSym64Rows = 2;      // rows per thread of the FP64 kernel
+constexpr int kSym64Threads = 256;  // -> the same 512-point blocks
+static_assert(kSym64Rows * kSym64Threads == kSymRows * kSymThreads,
+              "FP32 and FP64 symmetric kernels share their blocks and pair slots");
+
+template <int DP, bool CLAMP, bool BATCHED>
+cudaError_t launch_k4s_t(const double* E, int64_t n, const double* x, double* rowpart,
+                         double* colpart, const SymPlan& sp, const BatchMap& bm, int* status,
+                         const int* gate, cudaStream_t s) {
+  k4s_matvec_f64<DP, kSym64Rows, kSym64Threads, CLAMP, BATCHED>
+      <<<sp.grid, kSym64Threads, 0, s>>>(E, n, x, colpart, rowpart, sp, bm, status, gate);
+  return cudaGetLastError();
+}
+
+int k4s_occupancy(int dp) {
+  static int cache[9] = {};
+  if (dp < 2 || dp > 16) return 1;
+  int& c = cache[dp / 2];
+  if (c > 0) return c;
+  const void* fn = nullptr;
+#define LAKER_K4S_FN(DPv)                                                                 \
+  if (dp == DPv)                                                                          \
+    fn = reinterpret_cast<const void*>(&k4s_matvec_f64<DPv, kSym64Rows, kSym64Threads, false, false>);
+  LAKER_K4S_FN(2) LAKER_K4S_FN(4) LAKER_K4S_FN(6) LAKER_K4S_FN(8) LAKER_K4S_FN(10) LAKER_K4S_FN(12)
+  LAKER_K4S_FN(14) LAKER_K4S_FN(16)
+#undef LAKER_K4S_FN
+  int nb = 0;
+  if (!fn || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kSym64Threads, 0) != cudaSuccess ||
+      nb < 1) {
+    cudaGetLastError();
+    nb = 1;
+  }
+  c = nb;
+  return c;
+}
+
+__global__ void sym_finish_kernel(SymPlan sp, const double* __restrict__ rowpart,
                                   const float* __restrict__ colpart, int64_t n, float lam,
                                   const float* __restrict__ x, float* __restrict__ y, int64_t ldy) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
     y[i * ldy] = (float)((double)lam * (double)x[i] + sym_row_sum(sp, rowpart, colpart, i));
+}
+
+// y = [b -] (lam x + K64 x) from the FP64 kernel's partials.
+__global__ void sym_finish64_kernel(SymPlan sp, const double* __restrict__ rowpart,
+                                    const double* __restrict__ colpart, int64_t n, double lam,
+                                    const double* __restrict__ x, const double* __restrict__ b,
+                                    int64_t ldb, double* __restrict__ y, int64_t ldy) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double a = lam * x[i] + sym_row_sum(sp, rowpart, colpart, i);
+    y[i * ldy] = b ? b[i * ldb] - a : a;
+  }
 }
 
 }  // namespace
@@ -417,7 +645,7 @@ SymPlan k1s_plan(int64_t n, int d) {
 }
 
 cudaError_t launch_k1s(const float* E32, int64_t n, int d, int clamp, const float* x,
-                       float* rowpart, float* colpart, const SymPlan& sp, int* status,
+                       double* rowpart, float* colpart, const SymPlan& sp, int* status,
                        const int* gate, cudaStream_t s) {
   const int dp = padded_dim(d);
   const BatchMap none{};
@@ -430,7 +658,7 @@ cudaError_t launch_k1s(const float* E32, int64_t n, int d, int clamp, const floa
 }
 
 cudaError_t launch_k1s_batched(const float* E32, int d, int clamp, const float* x,
-                               float* rowpart, float* colpart, const SymPlan& sp,
+                               double* rowpart, float* colpart, const SymPlan& sp,
                                const BatchMap& bm, int* status, const int* gate, cudaStream_t s) {
   const int dp = padded_dim(d);
   if (clamp) {
@@ -441,7 +669,7 @@ cudaError_t launch_k1s_batched(const float* E32, int d, int clamp, const float* 
   return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_sym_finish(const SymPlan& sp, const float* rowpart, const float* colpart,
+cudaError_t launch_sym_finish(const SymPlan& sp, const double* rowpart, const float* colpart,
                               int64_t n, float lam, const float* x, float* y, int64_t ldy,
                               cudaStream_t s) {
   int g = (int)ceil_div(n, 256);
@@ -450,10 +678,72 @@ cudaError_t launch_sym_finish(const SymPlan& sp, const float* rowpart, const flo
   return cudaGetLastError();
 }
 
+SymPlan k4s_plan_pairs(int64_t nb, int64_t npairs, int d) {
+  SymPlan sp{};
+  sp.B = kSym64Rows * kSym64Threads;
+  sp.nb = nb;
+  sp.npairs = npairs;
+  const int64_t slots = (int64_t)sm_count() * k4s_occupancy(padded_dim(d));
+  sp.grid = (int)(npairs < slots ? (npairs > 0 ? npairs : 1) : slots);
+  sp.q = npairs / sp.grid;
+  sp.rem = npairs % sp.grid;
+  sp.cfg = 0;
+  return sp;
+}
+
+SymPlan k4s_plan(int64_t n, int d) {
+  const int B = kSym64Rows * kSym64Threads;
+  const int64_t nb = n > 0 ? ceil_div(n, B) : 1;
+  return k4s_plan_pairs(nb, nb * (nb + 1) / 2, d);
+}
+
+cudaError_t launch_k4s(const double* E64, int64_t n, int d, int clamp, const double* x,
+                       double* rowpart, double* colpart, const SymPlan& sp, int* status,
+                       const int* gate, cudaStream_t s) {
+  const int dp = padded_dim(d);
+  const BatchMap none{};
+  if (clamp) {
+    LAKER_DISPATCH_DPS(dp, return (launch_k4s_t<DPv, true, false>(E64, n, x, rowpart, colpart, sp, none, status, gate, s)));
+  } else {
+    LAKER_DISPATCH_DPS(dp, return (launch_k4s_t<DPv, false, false>(E64, n, x, rowpart, colpart, sp, none, status, gate, s)));
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_k4s_batched(const double* E64, int d, int clamp, const double* x,
+                               double* rowpart, double* colpart, const SymPlan& sp,
+                               const BatchMap& bm, int* status, const int* gate, cudaStream_t s) {
+  const int dp = padded_dim(d);
+  if (clamp) {
+    LAKER_DISPATCH_DPS(dp, return (launch_k4s_t<DPv, true, true>(E64, 0, x, rowpart, colpart, sp, bm, status, gate, s)));
+  } else {
+    LAKER_DISPATCH_DPS(dp, return (launch_k4s_t<DPv, false, true>(E64, 0, x, rowpart, colpart, sp, bm, status, gate, s)));
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_sym_finish64(const SymPlan& sp, const double* rowpart, const double* colpart,
+                                int64_t n, double lam, const double* x, const double* b,
+                                int64_t ldb, double* y, int64_t ldy, cudaStream_t s) {
+  int g = (int)ceil_div(n, 256);
+  if (g > sm_count() * 8) g = sm_count() * 8;
+  sym_finish64_kernel<<<g, 256, 0, s>>>(sp, rowpart, colpart, n, lam, x, b, ldb, y, ldy);
+  return cudaGetLastError();
+}
+
 bool k1_use_symmetric() {
   static int v = -1;
   if (v < 0) {
     const char* e = getenv("LAKER_K1_SYMMETRIC");
+    v = (e && e[0] == '0') ? 0 : 1;
+  }
+  return v == 1;
+}
+
+bool k4_use_symmetric() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("LAKER_K4_SYMMETRIC");
     v = (e && e[0] == '0') ? 0 : 1;
   }
   return v == 1;

@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(T)
 template <bool SYM>
 __global__ void __launch_bounds__(T)
     pcg_after_matvec_kernel(const double* __restrict__ part, int S, SymPlan sp,
-                            const float* __restrict__ rowpart,
+                            const double* __restrict__ rowpart,
                             const float* __restrict__ colpart, const float* __restrict__ p,
                             float* __restrict__ Ap, int64_t n, double* blockpart, PcgState* st) {
   if (st->done) return;
@@ -162,19 +162,28 @@ __global__ void __launch_bounds__(T)
   }
 }
 
-// After the FP64 matvec: r = b - (lam x + sum_s part[s]), |r| -> stop test.
-// `init` seeds the state for a warm start (no iteration has run yet).
+// After the FP64 matvec: r = b - (lam x + K64 x), |r| -> stop test.  SYM:
+// per-pair row and column sums of the symmetric FP64 kernel, else S
+// column-segment partials in `part`.  `init` seeds the state for a warm start
+// (no iteration has run yet).
+template <bool SYM>
 __global__ void __launch_bounds__(T)
-    pcg_after_residual_kernel(const double* __restrict__ part, int S, const double* __restrict__ b,
-                              const double* __restrict__ x, double* __restrict__ r, int64_t n,
-                              int init, double* blockpart, PcgState* st) {
+    pcg_after_residual_kernel(const double* __restrict__ part, int S, SymPlan sp,
+                              const double* __restrict__ rowpart, const double* __restrict__ colpart,
+                              const double* __restrict__ b, const double* __restrict__ x,
+                              double* __restrict__ r, int64_t n, int init, double* blockpart,
+                              PcgState* st) {
   if (st->done || (!init && !st->need_update)) return;
   __shared__ double s_red[T / 32];
   const double lam = st->lam;
   double acc = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)T + threadIdx.x; i < n; i += (int64_t)gridDim.x * T) {
     double a = lam * x[i];
-    for (int s = 0; s < S; ++s) a += part[(int64_t)s * n + i];
+    if (SYM) {
+      a += sym_row_sum(sp, rowpart, colpart, i);
+    } else {
+      for (int s = 0; s < S; ++s) a += part[(int64_t)s * n + i];
+    }
     const double ri = b[i] - a;
     r[i] = ri;
     acc = fma(ri, ri, acc);
@@ -318,10 +327,15 @@ PcgWs carve(void* base, int64_t n, int d, int nr) {
   {
     // FP32 matvec partials: column segments, or the symmetric kernel's layout
     size_t b32 = (size_t)p1.S * n * sizeof(double);
-    const size_t bs = sym_partial_bytes(k1s_plan(n, d));
+    const size_t bs = sym_partial_bytes<float>(k1s_plan(n, d));
     w.part32 = reinterpret_cast<double*>(take(b32 > bs ? b32 : bs));
   }
-  w.part64 = reinterpret_cast<double*>(take((size_t)p4.S * n * sizeof(double)));
+  {
+    // FP64 matvec partials: column segments, or the symmetric kernel's layout
+    const size_t b64 = (size_t)p4.S * n * sizeof(double);
+    const size_t bs = sym_partial_bytes<double>(k4s_plan(n, d));
+    w.part64 = reinterpret_cast<double*>(take(b64 > bs ? b64 : bs));
+  }
   w.blockpart = reinterpret_cast<double*>(take((size_t)G * 4 * sizeof(double)));
   (void)nr;  // the apply's partials are sized for the largest padded row (1024)
   w.upart = reinterpret_cast<double*>(take((size_t)precond_grid() * kMaxNr * sizeof(double)));
@@ -359,9 +373,30 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
   const SegPlan p1 = k1_plan(n, n, d), p4 = k4_plan(n, n, d);
   const bool sym = k1_use_symmetric();
   const SymPlan sp = k1s_plan(n, d);
-  float* sym_row = reinterpret_cast<float*>(w.part32);
-  float* sym_col = sym_colpart_ptr(w.part32, sp);
+  double* sym_row = w.part32;
+  float* sym_col = sym_colpart_ptr<float>(w.part32, sp);
   const int G = vec_grid(n), Gp = precond_grid();
+  int* dstatus = &w.hdr->status;
+  const bool sym64 = k4_use_symmetric();
+  const SymPlan sp64 = k4s_plan(n, d);
+  double* row64 = w.part64;
+  double* col64 = sym_colpart_ptr<double>(w.part64, sp64);
+  // r = b - A64 x (gated on the device by `gate`)
+  auto launch_residual = [&](int init, const int* gate) -> cudaError_t {
+    cudaError_t ee;
+    if (sym64) {
+      ee = launch_k4s(op->packed64, n, d, op->clamp, X, row64, col64, sp64, dstatus, gate, s);
+      if (ee == cudaSuccess)
+        pcg_after_residual_kernel<true><<<G, T, 0, s>>>(nullptr, 0, sp64, row64, col64, B, X, w.r,
+                                                        n, init, w.blockpart, w.st);
+    } else {
+      ee = launch_k4(op->packed64, n, op->packed64, n, d, op->clamp, X, w.part64, p4, dstatus, gate, s);
+      if (ee == cudaSuccess)
+        pcg_after_residual_kernel<false><<<G, T, 0, s>>>(w.part64, p4.S, sp64, nullptr, nullptr, B,
+                                                         X, w.r, n, init, w.blockpart, w.st);
+    }
+    return ee;
+  };
   const PcView view{pc ? pc->q_basis : nullptr, pc ? pc->w_core : nullptr, n, nr,
                     pc ? pc->ldq : 4, pc ? pc->inv_sqrt_iso : 1.0};
 
@@ -376,7 +411,6 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
   if (e == cudaSuccess) e = cudaMemcpyAsync(w.st, &h, sizeof(PcgState), cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return fail_cuda(e);
 
-  int* dstatus = &w.hdr->status;
   int launches = 0;
   LaunchTimer t32, t64;
   t32.init(prm->profile != 0);
@@ -402,9 +436,8 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
   if (e != cudaSuccess) return fail_cuda(e);
   if (prm->has_x0) {
     // warm start: r = b - A x0 with the FP64 operator (laker/solvers.py:165-173)
-    e = launch_k4(op->packed64, n, op->packed64, n, d, op->clamp, X, w.part64, p4, dstatus, nullptr, s);
+    e = launch_residual(1, nullptr);
     if (e != cudaSuccess) return fail_cuda(e);
-    pcg_after_residual_kernel<<<G, T, 0, s>>>(w.part64, p4.S, B, X, w.r, n, 1, w.blockpart, w.st);
     launches += 2;
   }
   e = cudaMemcpyAsync(&h, w.st, sizeof(PcgState), cudaMemcpyDeviceToHost, s);
@@ -456,10 +489,8 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
                                                        w.blockpart, w.st);
       pcg_update_xr_kernel<<<G, T, 0, s>>>(w.p, w.Ap, X, w.r, n, w.blockpart, w.st);
       t64.begin(s);
-      launch_k4(op->packed64, n, op->packed64, n, d, op->clamp, X, w.part64, p4, dstatus,
-                &w.st->need_update, s);
+      launch_residual(0, &w.st->need_update);
       t64.end(s);
-      pcg_after_residual_kernel<<<G, T, 0, s>>>(w.part64, p4.S, B, X, w.r, n, 0, w.blockpart, w.st);
       launches += 5;
       launch_precond(0);
     }

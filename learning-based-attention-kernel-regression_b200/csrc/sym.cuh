@@ -22,10 +22,12 @@ struct SymPlan {
 // Several independent problems in one launch: instance k owns the global
 // points [seg[k], seg[k] + npts[k]) (seg a multiple of 256, so its packed
 // embeddings start on a column tile), nblk[k] blocks and the global pairs
-// [pair_start[k], pair_start[k+1]); its blocks are global blocks
-// blk_start[k] .. blk_start[k+1]-1.  Pairs only pair blocks of the same
-// instance, so the operator is block diagonal.  done[k] != 0 skips an
-// instance (converged).  All arrays are device memory.
+// [pair_start[k], pair_start[k+1]) (the slots of its partial sums); its
+// blocks are global blocks blk_start[k] .. blk_start[k+1]-1.  Pairs only pair
+// blocks of the same instance, so the operator is block diagonal.  The launch
+// covers the running instances act_inst[0 .. *act_count), whose pairs are
+// numbered consecutively (act_ps, exclusive prefix sums) and split evenly over
+// the grid.  All arrays are device memory.
 struct BatchMap {
   int count;
   const int64_t* pair_start;  // [count + 1]
@@ -33,7 +35,9 @@ struct BatchMap {
   const int64_t* npts;        // [count]
   const int64_t* seg;         // [count]
   const int64_t* blk_start;   // [count + 1]
-  const int* done;            // [count] or null
+  const int* act_count;       // number of running instances
+  const int* act_inst;        // [count]
+  const int64_t* act_ps;      // [count + 1]
 };
 
 // Index of pair (a, b), a <= b, among the nb (nb + 1) / 2 pairs of nb blocks.
@@ -61,10 +65,12 @@ __host__ __device__ inline void sym_pair_coords(int64_t p, int64_t nb, int64_t* 
 // sum_j K_ij x_j for local row li of an instance whose pairs start at global
 // pair ps: the row sums of its pairs (a, b >= a), then the column sums of its
 // pairs (a' < a, a), in that fixed order.  Both partial arrays hold one
-// B-vector per pair.
+// B-vector per pair (FP32 kernel: double row sums, float column sums; FP64
+// kernel: both double).
+template <typename RP, typename CP>
 __device__ inline double sym_instance_row_sum(int64_t nb, int64_t ps, int B,
-                                              const float* __restrict__ rowpart,
-                                              const float* __restrict__ colpart, int64_t li) {
+                                              const RP* __restrict__ rowpart,
+                                              const CP* __restrict__ colpart, int64_t li) {
   const int64_t a = li / B, o = li - a * B;
   const int64_t f = ps + sym_first_pair(a, nb);
   double s = 0.0;
@@ -74,48 +80,72 @@ __device__ inline double sym_instance_row_sum(int64_t nb, int64_t ps, int B,
 }
 
 // Single instance.
-__device__ inline double sym_row_sum(const SymPlan& sp, const float* __restrict__ rowpart,
-                                     const float* __restrict__ colpart, int64_t i) {
-  return sym_instance_row_sum(sp.nb, 0, sp.B, rowpart, colpart, i);
+template <typename RP, typename CP>
+__device__ inline double sym_row_sum(const SymPlan& sp, const RP* __restrict__ rowpart,
+                                     const CP* __restrict__ colpart, int64_t i) {
+  return sym_instance_row_sum<RP, CP>(sp.nb, 0, sp.B, rowpart, colpart, i);
 }
 
 // Batched layout: local row li of instance k.
+template <typename RP, typename CP>
 __device__ inline double sym_row_sum_batched(const SymPlan& sp, const BatchMap& bm,
-                                             const float* __restrict__ rowpart,
-                                             const float* __restrict__ colpart, int k, int64_t li) {
-  return sym_instance_row_sum(bm.nblk[k], bm.pair_start[k], sp.B, rowpart, colpart, li);
+                                             const RP* __restrict__ rowpart,
+                                             const CP* __restrict__ colpart, int k, int64_t li) {
+  return sym_instance_row_sum<RP, CP>(bm.nblk[k], bm.pair_start[k], sp.B, rowpart, colpart, li);
 }
 
 // Points per block of the symmetric kernel.
 int sym_block_points();
 // Plan for n points of padded dimension from d.
 SymPlan k1s_plan(int64_t n, int d);
-// Plan for an explicit pair list (batched layout: nb = total blocks).
+// Plan for an explicit pair list (batched layout: nb = total blocks; the
+// batched kernel takes only the grid from it and splits the running pairs at
+// run time).
 SymPlan k1s_plan_pairs(int64_t nb, int64_t npairs, int d);
-// Workspace pieces: row and column partials, one B-vector of floats per pair.
+// Workspace pieces: row and column partials, one B-vector per pair.
 inline size_t sym_rowpart_elems(const SymPlan& sp) { return (size_t)sp.npairs * sp.B; }
 inline size_t sym_colpart_elems(const SymPlan& sp) { return (size_t)sp.npairs * sp.B; }
 cudaError_t launch_k1s(const float* E32, int64_t n, int d, int clamp, const float* x,
-                       float* rowpart, float* colpart, const SymPlan& sp, int* status,
+                       double* rowpart, float* colpart, const SymPlan& sp, int* status,
                        const int* gate, cudaStream_t s);
 cudaError_t launch_k1s_batched(const float* E32, int d, int clamp, const float* x,
-                               float* rowpart, float* colpart, const SymPlan& sp,
+                               double* rowpart, float* colpart, const SymPlan& sp,
                                const BatchMap& bm, int* status, const int* gate, cudaStream_t s);
 // y = lam x + (sum of the partials) for the standalone matvec.
-cudaError_t launch_sym_finish(const SymPlan& sp, const float* rowpart, const float* colpart,
+cudaError_t launch_sym_finish(const SymPlan& sp, const double* rowpart, const float* colpart,
                               int64_t n, float lam, const float* x, float* y, int64_t ldy,
                               cudaStream_t s);
 // Whether square FP32 matvecs use the symmetric kernel (LAKER_K1_SYMMETRIC=0
 // selects the plain one, for comparisons).
 bool k1_use_symmetric();
-// Bytes of the symmetric partials (rowpart, then colpart at a 256-byte boundary).
+// Bytes of the symmetric partials: row sums (double), then column sums (CP:
+// float for the FP32 kernel, double for the FP64 one) at a 256-byte boundary.
+template <typename CP>
 inline size_t sym_partial_bytes(const SymPlan& sp) {
-  return (size_t)round_up((int64_t)(sym_rowpart_elems(sp) * sizeof(float)), 256) +
-         sym_colpart_elems(sp) * sizeof(float);
+  return (size_t)round_up((int64_t)(sym_rowpart_elems(sp) * sizeof(double)), 256) +
+         sym_colpart_elems(sp) * sizeof(CP);
 }
-inline float* sym_colpart_ptr(void* partials, const SymPlan& sp) {
-  return reinterpret_cast<float*>(static_cast<char*>(partials) +
-                                  round_up((int64_t)(sym_rowpart_elems(sp) * sizeof(float)), 256));
+template <typename CP>
+inline CP* sym_colpart_ptr(void* partials, const SymPlan& sp) {
+  return reinterpret_cast<CP*>(static_cast<char*>(partials) +
+                               round_up((int64_t)(sym_rowpart_elems(sp) * sizeof(double)), 256));
 }
+
+// FP64 symmetric kernel (same blocks and pair slots; its own grid).
+SymPlan k4s_plan(int64_t n, int d);
+SymPlan k4s_plan_pairs(int64_t nb, int64_t npairs, int d);
+cudaError_t launch_k4s(const double* E64, int64_t n, int d, int clamp, const double* x,
+                       double* rowpart, double* colpart, const SymPlan& sp, int* status,
+                       const int* gate, cudaStream_t s);
+cudaError_t launch_k4s_batched(const double* E64, int d, int clamp, const double* x,
+                               double* rowpart, double* colpart, const SymPlan& sp,
+                               const BatchMap& bm, int* status, const int* gate, cudaStream_t s);
+// y = [b -] (lam x + K64 x) from the FP64 partials (b may be null).
+cudaError_t launch_sym_finish64(const SymPlan& sp, const double* rowpart, const double* colpart,
+                                int64_t n, double lam, const double* x, const double* b,
+                                int64_t ldb, double* y, int64_t ldy, cudaStream_t s);
+// Whether the FP64 residual uses the symmetric kernel (LAKER_K4_SYMMETRIC=0
+// selects the plain one).
+bool k4_use_symmetric();
 
 }  // namespace laker

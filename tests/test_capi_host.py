@@ -65,9 +65,11 @@ def test_workspace_and_layout_queries():
     offs = (ctypes.c_int64 * 4)()
     assert lib.laker_batch_layout(3, ns, offs) == 1024
     assert list(offs) == [0, 256, 512, 1024]
-    assert lib.laker_pcg_batched_workspace_bytes(3, ns, 6) > 1024 * 8
-    assert lib.laker_pcg_batched_workspace_bytes(3, ns, 17) == 0
-    assert lib.laker_pcg_batched_workspace_bytes(0, ns, 6) == 0
+    assert lib.laker_pcg_batched_workspace_bytes(3, ns, 6, 256) > 1024 * 8
+    assert lib.laker_pcg_batched_workspace_bytes(3, ns, 6, 0) > 1024 * 8
+    assert lib.laker_pcg_batched_workspace_bytes(3, ns, 6, 2000) == 0
+    assert lib.laker_pcg_batched_workspace_bytes(3, ns, 17, 0) == 0
+    assert lib.laker_pcg_batched_workspace_bytes(0, ns, 6, 0) == 0
     res = (_lib.laker_pcg_result * 3)()
     prm = _lib.laker_pcg_params(1e-6, 10, 0.1, 1e-8, 1, 0, 0)
     assert lib.laker_pcg_solve_batched(None, None, None, ctypes.byref(prm), None, 0, res,
