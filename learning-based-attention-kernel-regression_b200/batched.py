@@ -2,11 +2,12 @@
 
 `build_cccp_batched` builds the CCCP preconditioners of a list of operators
 (laker/preconditioner.py:144-284 per instance): probes, operator(probes) and
-QR per instance, then the N_r x N_r fixed point for all instances at once --
-padded to the largest N_r, batched float64 Cholesky on the GPU for
+CholeskyQR2 per instance, then the N_r x N_r fixed point for all instances at
+once -- padded to the largest N_r, batched float64 Cholesky on the GPU for
 diag(R^T M^-1 R) (the reference's eigh gives the same quantity; M is SPD), and
 a per-instance convergence mask that freezes each instance at the iteration the
-reference would stop at -- and a final per-instance eigh for the apply.
+reference would stop at -- and the apply's W = M^-1/2 - c^-1/2 I for all
+instances by a batched Newton-Schulz iteration.
 
 `BatchedPCG.solve` runs laker_pcg_solve_batched: one device loop for all
 instances (block-diagonal symmetric FP32 matvec over the block pairs of the
@@ -19,13 +20,15 @@ from __future__ import annotations
 
 import ctypes
 import logging
+import time
 from typing import List, Optional, Sequence
 
 import torch
 
 from . import _lib
 from .kernels import AttentionKernelOperator
-from .preconditioner import CCCPPreconditioner, adaptive_shrinkage_rho
+from .preconditioner import (CCCPPreconditioner, adaptive_shrinkage_rho, draw_probes,
+                             inv_sqrt_spd_batched, orthonormal_basis)
 
 logger = logging.getLogger(__name__)
 
@@ -39,37 +42,49 @@ def build_cccp_batched(
     max_iter: int = 200,
     tol: float = 1e-6,
     seeds: Optional[Sequence[int]] = None,
+    probe_device: Optional[torch.device] = None,
+    timings: Optional[dict] = None,
 ) -> List[CCCPPreconditioner]:
-    """CCCP preconditioners for many operators (one per operator)."""
+    """CCCP preconditioners for many operators (one per operator).
+
+    Instance k draws its probes like CCCPPreconditioner.build(seed=seeds[k])
+    (on the operator's device unless probe_device is given), so each result
+    matches the single build up to the float64 rounding of the batched fixed
+    point.  `timings`, when given, receives the seconds spent in each phase
+    (probes, operator, qr, fixed_point, apply_factors)."""
     count = len(operators)
     if count == 0:
         return []
     dev = operators[0].device
     f64 = torch.float64
+    clock = _PhaseClock(timings, dev)
     pres, rs, ns, nrs = [], [], [], []
     for k, op in enumerate(operators):
         n = op.n
         pre = CCCPPreconditioner(num_probes=num_probes, gamma=gamma, epsilon=epsilon,
                                  base_rho=base_rho, max_iter=max_iter, tol=tol, verbose=False,
-                                 device=dev, dtype=op.dtype)
+                                 device=dev, dtype=op.dtype, probe_device=probe_device)
         nr = num_probes if num_probes is not None else max(200, int(2 * n**0.5))
         nr = min(nr, n)
         if nr > 1024:
             raise ValueError(f"num_probes must be <= 1024 for the fused apply, got {nr}")
         pre.n, pre.nr = n, nr
-        gen = torch.Generator(device="cpu")
-        if seeds is not None:
-            gen.manual_seed(int(seeds[k]))
-        probes = torch.randn(n, nr, dtype=f64, generator=gen).to(dev, op.dtype)
+        clock.start()
+        probes = draw_probes(n, nr, op.dtype, pre.probe_device,
+                             seeds[k] if seeds is not None else None).to(dev)
+        clock.stop("probes")
         op_probes = op.matvec(probes).to(f64)
+        clock.stop("operator")
         norms = torch.linalg.norm(op_probes, dim=0, keepdim=True)
-        q, r = torch.linalg.qr(op_probes / norms.clamp(min=epsilon), mode="reduced")
+        q, r = orthonormal_basis(op_probes / norms.clamp(min=epsilon))
+        clock.stop("qr")
         pre.q_basis, pre.qr_r = q, r
         pres.append(pre)
         rs.append(r)
         ns.append(n)
         nrs.append(nr)
 
+    clock.start()
     m = max(nrs)
     R = torch.zeros(count, m, m, dtype=f64, device=dev)
     mask = torch.zeros(count, m, dtype=f64, device=dev)
@@ -108,28 +123,47 @@ def build_cccp_batched(
         qbm = torch.where(upd.view(-1, 1, 1), qbm_new, qbm)
         iters = iters + upd.to(torch.int64)
         active = active & ~(torch.maximum(iso_rel, q_rel) < tol)
-        if not bool(active.any()):
+        # converged instances are frozen by the mask, so polling every few
+        # iterations changes nothing but the number of host syncs
+        if it % 4 == 3 and not bool(active.any()):
             break
     iso_h = iso.tolist()
     iters_h = iters.tolist()
-    # final eigendecomposition per instance, grouped by N_r
-    by_nr = {}
+    clock.stop("fixed_point")
+    # W_k = (c_k I + B_k)^-1/2 - c_k^-1/2 I for the fused apply, for all
+    # instances at once: on the padded block c_k I the batched inverse square
+    # root is c_k^-1/2 I, so W vanishes there.  The eigen-decomposition (a
+    # reference state attribute) is computed only if it is read.
+    mm = eye * iso.view(-1, 1, 1) + qbm
+    W = inv_sqrt_spd_batched(mm) - eye * iso.rsqrt().view(-1, 1, 1)
     for k in range(count):
-        by_nr.setdefault(nrs[k], []).append(k)
-    for nr, ks in by_nr.items():
-        idx = torch.tensor(ks, device=dev)
-        mats = (torch.eye(nr, dtype=f64, device=dev) * iso[idx].view(-1, 1, 1)
-                + qbm[idx, :nr, :nr])
-        w, v = torch.linalg.eigh(mats)
-        w = w.clamp(min=epsilon)
-        for j, k in enumerate(ks):
-            pre = pres[k]
-            pre.isotropic_coef = float(iso_h[k])
-            pre.q_basis_matrix = qbm[k, :nr, :nr].clone()
-            pre.q_eigenvalues, pre.q_eigenvectors = w[j].clone(), v[j].clone()
-            pre.cccp_iterations = int(iters_h[k])
-            pre._prepare_apply()
+        pre = pres[k]
+        nr = nrs[k]
+        pre.isotropic_coef = float(iso_h[k])
+        pre.q_basis_matrix = qbm[k, :nr, :nr].clone()
+        pre.cccp_iterations = int(iters_h[k])
+        pre._prepare_apply(W[k, :nr, :nr])
+    clock.stop("apply_factors")
     return pres
+
+
+class _PhaseClock:
+    """Accumulates synchronised wall time per phase into a dict (or nothing)."""
+
+    def __init__(self, out: Optional[dict], device: torch.device) -> None:
+        self.out, self.device, self.t = out, device, 0.0
+
+    def start(self) -> None:
+        if self.out is not None:
+            torch.cuda.synchronize(self.device)
+            self.t = time.perf_counter()
+
+    def stop(self, phase: str) -> None:
+        if self.out is not None:
+            torch.cuda.synchronize(self.device)
+            now = time.perf_counter()
+            self.out[phase] = self.out.get(phase, 0.0) + now - self.t
+            self.t = now
 
 
 class BatchedPCG:

@@ -448,7 +448,10 @@ using namespace laker;
 
 extern "C" size_t laker_matvec_workspace_bytes(int64_t m, int64_t n, int d, int k, int precision) {
   if (m < 0 || n < 0 || d < 1 || d > 16 || k < 1) return 0;
-  if (k > 1) return kWsHeader;
+  if (k > 1) {
+    // the tensor-core path stages X as split, swizzled TF32 tiles
+    return kWsHeader + (k2_use_tensor_cores() && n > 0 ? (size_t)round_up((int64_t)k2_image_bytes(n, k), 256) : 0);
+  }
   const SegPlan p = precision == 64 ? k4_plan(m, n, d) : k1_plan(m, n, d);
   size_t bytes = (size_t)p.S * (size_t)m * sizeof(double);
   if (m == n && n > 0) {
@@ -474,7 +477,13 @@ extern "C" int laker_attn_matvec_f32(const float* rows32, int64_t m, const float
   cudaError_t e = cudaMemsetAsync(&hdr->status, 0, sizeof(int), s);
   if (e != cudaSuccess) return fail_cuda(e);
   if (k > 1) {
-    e = launch_multi_f32(rows32, m, cols32, n, d, (m == n) ? lam : 0.0f, clamp, X, k, ldx, Y, ldy, s);
+    if (k2_use_tensor_cores() && n > 0) {
+      uint8_t* img = reinterpret_cast<uint8_t*>(workspace) + kWsHeader;
+      e = launch_k2(rows32, m, cols32, n, d, clamp, (m == n) ? lam : 0.0f, X, ldx, k, Y, ldy, img,
+                    &hdr->status, s);
+    } else {
+      e = launch_multi_f32(rows32, m, cols32, n, d, (m == n) ? lam : 0.0f, clamp, X, k, ldx, Y, ldy, s);
+    }
     return e == cudaSuccess ? LAKER_OK : fail_cuda(e);
   }
   // Single RHS: strided x is staged element-wise; a contiguous copy is not needed.

@@ -9,8 +9,11 @@ P = c^-1/2 I + Q V diag(lambda^-1/2 - c^-1/2) V^T Q^T is folded into
 W = V diag(lambda^-1/2 - c^-1/2) V^T (symmetrised) and applied by the fused
 two-pass kernel (laker_precond_apply), which the fused PCG also uses.
 
-Probe draws come from a CPU generator (moved to the device), so a seeded build
-matches the CPU float64 oracle; the reference draws on the target device.
+Probes are drawn as the reference draws them (laker/preconditioner.py:168-171):
+torch.randn in the preconditioner's dtype from a generator on its device, so a
+seeded build on a CUDA device sees the probes the reference sees on that
+device.  probe_device="cpu" draws from a CPU generator instead, which
+reproduces a reference build run on the CPU (the float64 goldens).
 """
 
 from __future__ import annotations
@@ -42,6 +45,56 @@ def eigh_stable(mat: torch.Tensor, eps: float = 1e-10):
     return w.clamp(min=eps), v
 
 
+def draw_probes(n: int, nr: int, dtype: torch.dtype, device: torch.device,
+                seed: Optional[int]) -> torch.Tensor:
+    """Gaussian probes U (n, N_r) as laker/preconditioner.py:168-171 draws them."""
+    gen = torch.Generator(device=device)
+    if seed is not None:
+        gen.manual_seed(int(seed))
+    return torch.randn(n, nr, device=device, dtype=dtype, generator=gen)
+
+
+def orthonormal_basis(U: torch.Tensor):
+    """Economy QR U = Q R of a tall float64 matrix (laker/preconditioner.py:191).
+
+    CholeskyQR2 (two passes of G = Q^T Q, G = L L^T, Q <- Q L^-T; R = R2 R1):
+    two GEMMs and two triangular solves instead of Householder QR, orthogonal
+    to rounding while cond(U) < ~1e8.  Householder QR (torch.linalg.qr) is the
+    fallback when a Cholesky factorisation fails.  R has a positive diagonal,
+    so Q and R can differ from Householder's by column signs Q D, D R; the CCCP
+    weights diag(R^T M^-1 R) and the apply Q V f(Lambda) V^T Q^T do not see D.
+    """
+    Q, R = U, None
+    for _ in range(2):
+        L, info = torch.linalg.cholesky_ex(Q.T @ Q)
+        if int(info.item()) != 0:
+            return torch.linalg.qr(U, mode="reduced")
+        Q = torch.linalg.solve_triangular(L.T, Q, upper=True, left=False)
+        R = L.T if R is None else L.T @ R
+    return Q, R
+
+
+def inv_sqrt_spd_batched(M: torch.Tensor, max_iter: int = 100, tol: float = 1e-14) -> torch.Tensor:
+    """M^{-1/2} for a batch of SPD float64 matrices (B, m, m).
+
+    Coupled Newton-Schulz iteration on M / s with s = ||M||_F >= lambda_max:
+    T = (3 I - Z Y) / 2, Y <- Y T, Z <- T Z, so Z -> (M / s)^{-1/2}; only
+    batched GEMMs, no eigensolver.  Stops when every ||I - Z Y||_F <= tol.
+    """
+    s = torch.linalg.matrix_norm(M).clamp(min=1e-300)
+    eye = torch.eye(M.shape[-1], dtype=M.dtype, device=M.device).expand_as(M)
+    Y = M / s.view(-1, 1, 1)
+    Z = eye.clone()
+    for it in range(max_iter):
+        ZY = Z @ Y
+        if it % 4 == 0 and float(torch.linalg.matrix_norm(eye - ZY).max()) <= tol:
+            break
+        T = 1.5 * eye - 0.5 * ZY
+        Y = Y @ T
+        Z = T @ Z
+    return Z / s.sqrt().view(-1, 1, 1)
+
+
 def preconditioner_apply_core(x, isotropic_coef, q_basis, q_eigenvalues, q_eigenvectors):
     """Unfused reference form of the apply (laker/preconditioner.py:52-68)."""
     inv = isotropic_coef ** (-0.5)
@@ -68,6 +121,7 @@ class CCCPPreconditioner:
         dtype: Optional[torch.dtype] = None,
         probe_strategy: str = "gaussian",
         power_iter_steps: int = 3,
+        probe_device: Optional[torch.device] = None,
     ) -> None:
         self.num_probes = num_probes
         self.gamma = float(gamma)
@@ -80,14 +134,14 @@ class CCCPPreconditioner:
         self.power_iter_steps = int(power_iter_steps)
         self.device = torch.device(device) if device is not None else get_default_device()
         self.dtype = dtype if dtype is not None else get_default_dtype()
+        self.probe_device = torch.device(probe_device) if probe_device is not None else self.device
         self.n: Optional[int] = None
         self.nr: Optional[int] = None
         self.q_basis: Optional[torch.Tensor] = None
         self.qr_r: Optional[torch.Tensor] = None
         self.isotropic_coef: Optional[float] = None
         self.q_basis_matrix: Optional[torch.Tensor] = None
-        self.q_eigenvalues: Optional[torch.Tensor] = None
-        self.q_eigenvectors: Optional[torch.Tensor] = None
+        self._q_eig = None  # (eigenvalues, eigenvectors) of c I + B, computed on demand
         self.cccp_iterations: int = 0
         self._q32: Optional[torch.Tensor] = None
         self._w32: Optional[torch.Tensor] = None
@@ -108,12 +162,7 @@ class CCCPPreconditioner:
         if self.verbose:
             logger.info("Building CCCP preconditioner: n=%d, N_r=%d", n, self.nr)
 
-        gen = torch.Generator(device="cpu")
-        if seed is not None:
-            gen.manual_seed(seed)
-        # drawn in float64 (as the float64 reference does) and cast to the
-        # operator dtype, so a float32 build sees the same directions
-        probes = torch.randn(n, self.nr, dtype=torch.float64, generator=gen).to(dev, dt)
+        probes = draw_probes(n, self.nr, dt, self.probe_device, seed).to(dev)
 
         if self.probe_strategy == "power_iter":
             n_power = max(1, int(self.nr * 0.25))
@@ -129,7 +178,7 @@ class CCCPPreconditioner:
         dt = torch.float64
         norms = torch.linalg.norm(op_probes, dim=0, keepdim=True)
         normalized = op_probes / norms.clamp(min=self.epsilon)
-        q_basis, qr_r = torch.linalg.qr(normalized, mode="reduced")
+        q_basis, qr_r = orthonormal_basis(normalized)
         self.q_basis, self.qr_r = q_basis, qr_r
 
         shrinkage = adaptive_shrinkage_rho(self.nr, n, self.gamma, self.base_rho)
@@ -172,10 +221,37 @@ class CCCPPreconditioner:
             logger.info("CCCP preconditioner built in %d iterations", it + 1)
         return self
 
-    def _prepare_apply(self) -> None:
-        v = self.q_eigenvectors.to(torch.float64)
-        scale = self.q_eigenvalues.to(torch.float64).rsqrt() - self.isotropic_coef ** (-0.5)
-        w = (v * scale.unsqueeze(0)) @ v.T
+    # eigen-decomposition of c I + B (reference state attributes); a batched
+    # build leaves it to be computed on first access
+    @property
+    def q_eigenvalues(self) -> Optional[torch.Tensor]:
+        return self._eig()[0]
+
+    @q_eigenvalues.setter
+    def q_eigenvalues(self, value) -> None:
+        self._q_eig = (value, self._q_eig[1] if self._q_eig else None)
+
+    @property
+    def q_eigenvectors(self) -> Optional[torch.Tensor]:
+        return self._eig()[1]
+
+    @q_eigenvectors.setter
+    def q_eigenvectors(self, value) -> None:
+        self._q_eig = (self._q_eig[0] if self._q_eig else None, value)
+
+    def _eig(self):
+        if (self._q_eig is None or self._q_eig[0] is None) and self.q_basis_matrix is not None:
+            eye = torch.eye(self.nr, device=self.q_basis_matrix.device, dtype=self.q_basis_matrix.dtype)
+            self._q_eig = eigh_stable(eye * self.isotropic_coef + self.q_basis_matrix, eps=self.epsilon)
+        return self._q_eig if self._q_eig is not None else (None, None)
+
+    def _prepare_apply(self, w: Optional[torch.Tensor] = None) -> None:
+        """Fold the apply into (Q padded, W = V diag(lambda^-1/2 - c^-1/2) V^T);
+        a batched build passes W computed as (c I + B)^-1/2 - c^-1/2 I."""
+        if w is None:
+            v = self.q_eigenvectors.to(torch.float64)
+            scale = self.q_eigenvalues.to(torch.float64).rsqrt() - self.isotropic_coef ** (-0.5)
+            w = (v * scale.unsqueeze(0)) @ v.T
         w = 0.5 * (w + w.T)
         self._q32 = _lib.padded_q(self.q_basis)
         self._w32 = w.to(torch.float32).contiguous()

@@ -1,8 +1,9 @@
 """GPU parity of the fused kernels against the float64 oracle and the goldens.
 
 Tolerances: the FP32 operator carries FP32 entries (ex2.approx, FP32 logits),
-so it is held to 3e-5 relative per output (the reference's own float32 test
-tolerance is rtol 1e-4); FP64 kernels are held to 1e-12.
+so it is held to 3e-5 relative per output; its multi-RHS form contracts on the
+tensor cores in split TF32 (~2^-21 per product) and is held to the reference's
+own float32 test tolerance, 1e-4; FP64 kernels are held to 1e-12.
 """
 
 import numpy as np
@@ -14,6 +15,7 @@ from oracle import laker_oracle as O
 pytestmark = pytest.mark.gpu
 
 F32_RTOL = 3e-5
+F32_MULTI_RTOL = 1e-4
 F64_RTOL = 1e-12
 
 
@@ -34,7 +36,7 @@ def test_matvec_golden(cuda, golden, key):
         x = torch.tensor(g[f"{key}_x"], device=cuda, dtype=dtype)
         X = torch.tensor(g[f"{key}_X"], device=cuda, dtype=dtype)
         assert rel(op.matvec(x), g[f"{key}_matvec"]) < tol
-        assert rel(op.matvec(X), g[f"{key}_matvec2d"]) < tol
+        assert rel(op.matvec(X), g[f"{key}_matvec2d"]) < (F32_MULTI_RTOL if dtype == torch.float32 else tol)
         assert rel(op.diagonal(), g[f"{key}_diag"]) < max(tol, 1e-6 if dtype == torch.float32 else 0)
         q = torch.tensor(g[f"{key}_q"], device=cuda, dtype=dtype)
         assert rel(op.kernel_eval(q), g[f"{key}_keval"]) < max(tol, 1e-6 if dtype == torch.float32 else 0)
@@ -73,7 +75,7 @@ def test_matvec_all_dims(cuda, d):
                O.attention_matvec(E, 0.02, x)) < F32_RTOL
     assert rel(op64.matvec(torch.tensor(x, device=cuda)), O.attention_matvec(E, 0.02, x)) < F64_RTOL
     assert rel(op32.matvec(torch.tensor(X, device=cuda, dtype=torch.float32)),
-               O.attention_matvec(E, 0.02, X)) < F32_RTOL
+               O.attention_matvec(E, 0.02, X)) < F32_MULTI_RTOL
     assert rel(op64.matvec(torch.tensor(X, device=cuda)), O.attention_matvec(E, 0.02, X)) < F64_RTOL
 
 
@@ -89,7 +91,7 @@ def test_matvec_multi_rhs_wide(cuda):
     op32 = AttentionKernelOperator(torch.tensor(E, device=cuda), lambda_reg=0.01)
     Y = op32.matvec(torch.tensor(X, device=cuda, dtype=torch.float32))
     col = [rel(Y[:, c], ref[:, c]) for c in range(k)]
-    assert max(col) < F32_RTOL
+    assert max(col) < F32_MULTI_RTOL
     op64 = AttentionKernelOperator(torch.tensor(E, device=cuda).double(), lambda_reg=0.01)
     assert rel(op64.matvec(torch.tensor(X, device=cuda)), ref) < F64_RTOL
 
@@ -141,8 +143,9 @@ def test_precond_apply_golden(cuda, golden):
     g = golden("solver_n400")
     E = torch.tensor(g["E"], device=cuda)
     op = AttentionKernelOperator(E, lambda_reg=float(g["lam"]))
+    # probes from a CPU generator: the golden comes from the reference run on the CPU
     pre = CCCPPreconditioner(num_probes=60, gamma=0.1, max_iter=50, tol=1e-6, verbose=False,
-                             device=cuda, dtype=torch.float64)
+                             device=cuda, dtype=torch.float64, probe_device="cpu")
     pre.build(op.matvec, E.shape[0], seed=3)
     assert abs(pre.isotropic_coef - float(g["iso"])) < 1e-8 * float(g["iso"])
     assert rel(pre.q_eigenvalues, g["q_eigenvalues"]) < 1e-8
