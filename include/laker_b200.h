@@ -47,8 +47,9 @@ enum laker_status {
   LAKER_ERR_TIMEOUT = 6,       /* a bounded device wait expired              */
   LAKER_ERR_WORKSPACE = 7,     /* workspace smaller than the query returned  */
   LAKER_ERR_UNSUPPORTED = 8,   /* shape/dtype combination not implemented    */
-  LAKER_ERR_SCRATCH_LIMIT = 9  /* larger than the fixed scratch of the
+  LAKER_ERR_SCRATCH_LIMIT = 9, /* larger than the fixed scratch of the
                                   allocation-free entry point               */
+  LAKER_ERR_CAPACITY = 10      /* engine: no free slot, points or pairs      */
 };
 
 /* Library version as 10000*major + 100*minor + patch. */
@@ -228,8 +229,74 @@ int laker_pcg_solve(const laker_operator* op, const laker_precond* pc, const dou
                     size_t workspace_bytes, laker_pcg_result* result, void* stream);
 
 /* ------------------------------------------------------------------------ */
-/* Batched PCG: many independent regressions in one solve                    */
+/* Solve engine: many independent regressions in one device loop            */
 /* ------------------------------------------------------------------------ */
+/* A persistent device loop over resident instances ("slots").  Per
+ * iteration: one symmetric FP32 matvec launch over the block pairs of the
+ * running instances (the list is compacted on the device after every
+ * iteration, so the whole grid works on what is left), vector kernels over
+ * the 512-point blocks of every running instance with per-instance reductions
+ * in a fixed order, and a symmetric FP64 residual over the instances whose
+ * recurrence asked for one; scalars and convergence masks live on the device
+ * and the iteration is captured once as a CUDA graph.  Instances are admitted
+ * and collected between graph replays (continuous batching); an instance's
+ * result does not depend on the other instances in the engine.  The caller
+ * owns both the host state buffer and the device workspace; the engine
+ * allocates nothing.  One host thread drives an engine.
+ * Replaces loops of PreconditionedConjugateGradient.solve calls
+ * (laker/solvers.py:130-295) over independent problems; the reference has no
+ * engine of its own. */
+typedef struct laker_engine_config {
+  int max_slots;       /* instances resident at once                            */
+  int64_t max_points;  /* sum over resident instances of round_up(n, 512)       */
+  int64_t max_pairs;   /* sum over resident instances of nb (nb + 1) / 2,
+                          nb = ceil(n / 512)                                    */
+  int d;               /* embedding dimension (all instances)                   */
+  int max_nr;          /* largest preconditioner N_r (0: none)                  */
+  int clamp;           /* 1: clamp Gram entries (needed when any instance's
+                          operator does not skip the clamp)                     */
+  int chunk;           /* iterations per graph replay (>= 1)                    */
+} laker_engine_config;
+
+size_t laker_engine_host_bytes(const laker_engine_config* cfg);
+size_t laker_engine_workspace_bytes(const laker_engine_config* cfg);
+
+/* Sets up an engine in `host` (host memory, laker_engine_host_bytes) over
+ * `workspace` (device memory, laker_engine_workspace_bytes).  params: tol,
+ * max_iter, reliable_delta, breakdown_eps as for laker_pcg_solve (has_x0
+ * must be 0).  All later calls enqueue on `stream`. */
+int laker_engine_init(void* host, size_t host_bytes, void* workspace, size_t workspace_bytes,
+                      const laker_engine_config* cfg, const laker_pcg_params* params,
+                      void* stream);
+
+/* Admits one instance: n points, lambda, its packed32 / packed64 embeddings
+ * (laker_pack_f32 / _f64 layouts, DEVICE), preconditioner (HOST struct of
+ * device factors, or NULL) and right-hand side b (DEVICE, n doubles).  The
+ * embeddings and b are copied into the engine; the factors must stay alive
+ * until the instance is collected.  Writes the slot index to *slot.
+ * LAKER_ERR_CAPACITY when no slot, points or pairs are free (after
+ * compacting the resident instances). */
+int laker_engine_admit(void* host, int64_t n, double lambda_reg, const float* packed32,
+                       const double* packed64, const laker_precond* pc, const double* b,
+                       int* slot);
+
+/* Runs one graph replay (cfg.chunk iterations of every running instance) and
+ * waits for it.  *running: instances still iterating afterwards. */
+int laker_engine_step(void* host, int* running);
+
+/* Slots that have stopped (converged, failed or hit max_iter) and are not yet
+ * collected: up to max_slots of them into slots[], their number in *count. */
+int laker_engine_finished(void* host, int* slots, int max_slots, int* count);
+
+/* Copies the solution of a stopped slot to x (DEVICE, n doubles), fills
+ * *result and frees the slot. */
+int laker_engine_collect(void* host, int slot, double* x, laker_pcg_result* result);
+
+/* Releases the engine's CUDA graph and private stream (the host and device
+ * buffers stay the caller's). */
+int laker_engine_release(void* host);
+
+/* ---- one-shot batch on top of the engine ------------------------------- */
 /* Instance k has n[k] points; every batched vector and packed buffer holds
  * instance k at points [offsets[k], offsets[k] + n[k]) with offsets[0] = 0 and
  * offsets[k+1] = offsets[k] + round_up(n[k], 256) (zero padding between).
@@ -251,23 +318,16 @@ typedef struct laker_batch {
 } laker_batch;
 
 /* Workspace for a batch whose preconditioners have at most max_nr probes
- * (0: no preconditioner); 0 for invalid sizes. */
+ * (0: no preconditioner); 0 for invalid sizes.  Includes the engine's
+ * workspace and a host-state area at its end. */
 size_t laker_pcg_batched_workspace_bytes(int count, const int64_t* n, int d, int max_nr);
 
-/* Solves A_k x_k = b_k for every instance with the mixed-precision PCG of
- * laker_pcg_solve in one device loop.  Per iteration: one symmetric FP32
- * matvec launch over the block pairs of the instances still running (the list
- * is compacted on the device after every iteration, so the whole grid works on
- * what is left), then vector kernels with one CTA per 512-point block of every
- * running instance and per-instance reductions in a fixed order; scalars and
- * convergence masks live on the device and the iteration is captured once as a
- * CUDA graph and replayed until every instance has stopped.  An instance's
- * result does not depend on the other instances of the batch.  B, X: batched
- * vectors (padded length).  results: HOST array of count results.  Returns
- * LAKER_OK unless a call failed; per-instance outcomes are in
- * results[k].status.  Warm starts (has_x0) are not supported.
- * Replaces a loop of PreconditionedConjugateGradient.solve calls
- * (laker/solvers.py:130-295) over independent problems. */
+/* Solves A_k x_k = b_k for every instance: one engine sized for the batch,
+ * every instance admitted, steps until all have stopped, every instance
+ * collected.  B, X: batched vectors (padded length).  results: HOST array of
+ * count results.  Returns LAKER_OK unless a call failed; per-instance
+ * outcomes are in results[k].status.  Warm starts (has_x0) are not
+ * supported. */
 int laker_pcg_solve_batched(const laker_batch* batch, const double* B, double* X,
                             const laker_pcg_params* params, void* workspace,
                             size_t workspace_bytes, laker_pcg_result* results, void* stream);

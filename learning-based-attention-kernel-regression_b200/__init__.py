@@ -27,6 +27,7 @@ from .models import LAKERRegressor
 from .preconditioner import CCCPPreconditioner, adaptive_shrinkage_rho, eigh_stable
 from .solvers import PreconditionedConjugateGradient
 from .batched import BatchedPCG, build_cccp_batched
+from .engine import EngineCapacityError, SolveEngine, engine_bytes_per_instance
 
 __version__ = "0.1.0"
 
@@ -43,6 +44,9 @@ __all__ = [
     "BatchedPCG",
     "build_cccp_batched",
     "CCCPPreconditioner",
+    "EngineCapacityError",
+    "SolveEngine",
+    "engine_bytes_per_instance",
     "KernelOperator",
     "LAKERCore",
     "LAKERRegressor",

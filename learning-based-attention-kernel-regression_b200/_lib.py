@@ -33,6 +33,7 @@ LAKER_ERR_TIMEOUT = 6
 LAKER_ERR_WORKSPACE = 7
 LAKER_ERR_UNSUPPORTED = 8
 LAKER_ERR_SCRATCH_LIMIT = 9
+LAKER_ERR_CAPACITY = 10
 
 
 class LakerError(RuntimeError):
@@ -106,8 +107,33 @@ class laker_batch(ctypes.Structure):
     ]
 
 
+class laker_engine_config(ctypes.Structure):
+    _fields_ = [
+        ("max_slots", c_int),
+        ("max_points", c_int64),
+        ("max_pairs", c_int64),
+        ("d", c_int),
+        ("max_nr", c_int),
+        ("clamp", c_int),
+        ("chunk", c_int),
+    ]
+
+
 _P = c_void_p
 _SIGNATURES = {
+    "laker_engine_host_bytes": (c_size_t, [POINTER(laker_engine_config)]),
+    "laker_engine_workspace_bytes": (c_size_t, [POINTER(laker_engine_config)]),
+    "laker_engine_init": (
+        c_int,
+        [_P, c_size_t, _P, c_size_t, POINTER(laker_engine_config), POINTER(laker_pcg_params), _P],
+    ),
+    "laker_engine_admit": (
+        c_int, [_P, c_int64, c_double, _P, _P, POINTER(laker_precond), _P, POINTER(c_int)],
+    ),
+    "laker_engine_step": (c_int, [_P, POINTER(c_int)]),
+    "laker_engine_finished": (c_int, [_P, POINTER(c_int), c_int, POINTER(c_int)]),
+    "laker_engine_collect": (c_int, [_P, c_int, _P, POINTER(laker_pcg_result)]),
+    "laker_engine_release": (c_int, [_P]),
     "laker_batch_layout": (c_int64, [c_int, POINTER(c_int64), POINTER(c_int64)]),
     "laker_pcg_batched_workspace_bytes": (c_size_t, [c_int, POINTER(c_int64), c_int, c_int]),
     "laker_pcg_solve_batched": (

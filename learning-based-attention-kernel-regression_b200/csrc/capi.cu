@@ -156,6 +156,7 @@ extern "C" const char* laker_status_string(int status) {
     case LAKER_ERR_TIMEOUT: return "bounded device wait expired";
     case LAKER_ERR_WORKSPACE: return "workspace too small";
     case LAKER_ERR_UNSUPPORTED: return "unsupported shape or dtype";
+    case LAKER_ERR_CAPACITY: return "engine capacity exhausted (slots, points or block pairs)";
     case LAKER_ERR_SCRATCH_LIMIT:
       return "problem larger than the fixed scratch of the allocation-free entry point "
              "(m > LAKER_NOALLOC_MAX_ROWS)";

@@ -44,14 +44,14 @@ template <bool BATCHED>
 __device__ __forceinline__ void cursor_load_inst(SymCursor& cu, const SymPlan& sp,
                                                  const BatchMap& bm, int64_t n) {
   if (BATCHED) {
-    const int k = bm.act_inst[cu.j];
-    cu.nb = bm.nblk[k];
-    cu.npts = bm.npts[k];
-    cu.seg = bm.seg[k];
-    cu.blk0 = bm.blk_start[k];
+    const SlotInfo& si = bm.slots[bm.act_inst[cu.j]];
+    cu.nb = si.nblk;
+    cu.npts = si.npts;
+    cu.seg = si.seg;
+    cu.blk0 = si.blk_start;
     cu.pstart = bm.act_ps[cu.j];
     cu.pend = bm.act_ps[cu.j + 1];
-    cu.gp0 = bm.pair_start[k];
+    cu.gp0 = si.pair_start;
   } else {
     cu.nb = sp.nb;
     cu.npts = n;

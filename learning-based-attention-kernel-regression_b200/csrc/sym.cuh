@@ -19,25 +19,28 @@ struct SymPlan {
   int cfg;         // kernel variant
 };
 
-// Several independent problems in one launch: instance k owns the global
-// points [seg[k], seg[k] + npts[k]) (seg a multiple of 256, so its packed
-// embeddings start on a column tile), nblk[k] blocks and the global pairs
-// [pair_start[k], pair_start[k+1]) (the slots of its partial sums); its
-// blocks are global blocks blk_start[k] .. blk_start[k+1]-1.  Pairs only pair
-// blocks of the same instance, so the operator is block diagonal.  The launch
-// covers the running instances act_inst[0 .. *act_count), whose pairs are
-// numbered consecutively (act_ps, exclusive prefix sums) and split evenly over
-// the grid.  All arrays are device memory.
+// Placement of one instance of a batched launch: its points [seg, seg + npts)
+// (seg a multiple of 512, so its packed embeddings start on a column tile and
+// its blocks are whole), blocks blk_start .. blk_start + nblk - 1 and block
+// pairs pair_start .. pair_start + nblk (nblk + 1) / 2 - 1 (the slots of its
+// partial sums).  Pairs only pair blocks of the same instance, so the
+// operator is block diagonal.
+struct SlotInfo {
+  int64_t seg, npts, nblk, blk_start, pair_start;
+  double lam, cis;  // lambda, c^-1/2 of the preconditioner
+  uint64_t q, w;    // preconditioner factors (0: none)
+  int nr, ldq;
+};
+
+// Several independent problems in one launch: slot k is described by
+// slots[k]; the launch covers the instances act_inst[0 .. *act_count), whose
+// pairs are numbered consecutively (act_ps, exclusive prefix sums) and split
+// evenly over the grid.  All arrays are device memory.
 struct BatchMap {
-  int count;
-  const int64_t* pair_start;  // [count + 1]
-  const int64_t* nblk;        // [count]
-  const int64_t* npts;        // [count]
-  const int64_t* seg;         // [count]
-  const int64_t* blk_start;   // [count + 1]
-  const int* act_count;       // number of running instances
-  const int* act_inst;        // [count]
-  const int64_t* act_ps;      // [count + 1]
+  const SlotInfo* slots;
+  const int* act_count;   // number of instances in the launch
+  const int* act_inst;    // their slots
+  const int64_t* act_ps;  // [count + 1]
 };
 
 // Index of pair (a, b), a <= b, among the nb (nb + 1) / 2 pairs of nb blocks.
@@ -91,7 +94,8 @@ template <typename RP, typename CP>
 __device__ inline double sym_row_sum_batched(const SymPlan& sp, const BatchMap& bm,
                                              const RP* __restrict__ rowpart,
                                              const CP* __restrict__ colpart, int k, int64_t li) {
-  return sym_instance_row_sum<RP, CP>(bm.nblk[k], bm.pair_start[k], sp.B, rowpart, colpart, li);
+  return sym_instance_row_sum<RP, CP>(bm.slots[k].nblk, bm.slots[k].pair_start, sp.B, rowpart,
+                                      colpart, li);
 }
 
 // Points per block of the symmetric kernel.
