@@ -284,6 +284,15 @@ int laker_engine_admit(void* host, int64_t n, double lambda_reg, const float* pa
  * waits for it.  *running: instances still iterating afterwards. */
 int laker_engine_step(void* host, int* running);
 
+/* laker_engine_step in two halves: _launch enqueues the replay and the read
+ * back of the engine's flags into the host state, _sync waits for them and
+ * updates the stopped slots; admit and collect are refused in between.
+ * _launch returns at once only when the host state buffer is pinned
+ * (cudaHostAlloc / cudaHostRegister); with pageable memory the read back
+ * makes it wait for the replay. */
+int laker_engine_launch(void* host);
+int laker_engine_sync(void* host, int* running);
+
 /* Slots that have stopped (converged, failed or hit max_iter) and are not yet
  * collected: up to max_slots of them into slots[], their number in *count. */
 int laker_engine_finished(void* host, int* slots, int max_slots, int* count);

@@ -131,6 +131,8 @@ _SIGNATURES = {
         c_int, [_P, c_int64, c_double, _P, _P, POINTER(laker_precond), _P, POINTER(c_int)],
     ),
     "laker_engine_step": (c_int, [_P, POINTER(c_int)]),
+    "laker_engine_launch": (c_int, [_P]),
+    "laker_engine_sync": (c_int, [_P, POINTER(c_int)]),
     "laker_engine_finished": (c_int, [_P, POINTER(c_int), c_int, POINTER(c_int)]),
     "laker_engine_collect": (c_int, [_P, c_int, _P, POINTER(laker_pcg_result)]),
     "laker_engine_release": (c_int, [_P]),

@@ -584,6 +584,8 @@ struct EngineHost {
   SymPlan sp32, sp64;
   int block_grid;
   int running;
+  int launched;      // a replay is in flight (laker_engine_launch)
+  int readback[2];   // running count, device status of the last replay
   int64_t nb_used, pairs_used;
   SlotHost* slots;  // [max_slots], in the host buffer after this struct
   int* done_h;      // [max_slots]
@@ -835,6 +837,7 @@ extern "C" int laker_engine_admit(void* host, int64_t n, double lambda_reg, cons
                                   int* slot) {
   EngineHost* e = engine_of(host);
   if (!e || n < 1 || !packed32 || !packed64 || !b || !slot) return LAKER_ERR_INVALID_ARG;
+  if (e->launched) return LAKER_ERR_INVALID_ARG;  // between replays only
   if (pc && (pc->n != n || pc->nr < 1 || pc->nr > e->cfg.max_nr || pc->ldq < pc->nr ||
              pc->ldq > e->L.ustride || (pc->ldq % 4) || !pc->q_basis || !pc->w_core ||
              (reinterpret_cast<uintptr_t>(pc->q_basis) % 16)))
@@ -908,26 +911,50 @@ extern "C" int laker_engine_admit(void* host, int64_t n, double lambda_reg, cons
   return LAKER_OK;
 }
 
-extern "C" int laker_engine_step(void* host, int* running) {
+extern "C" int laker_engine_launch(void* host) {
   EngineHost* e = engine_of(host);
-  if (!e || !running) return LAKER_ERR_INVALID_ARG;
+  if (!e) return LAKER_ERR_INVALID_ARG;
+  if (e->launched) return LAKER_ERR_INVALID_ARG;
   const EngineLayout& L = e->L;
+  // the replay, then the running count, stop flags and device status into
+  // the host state (pageable: the copies complete before laker_engine_sync
+  // returns)
   cudaError_t err = cudaGraphLaunch(e->exec, e->stream);
-  int active = 0, status = 0;
   if (err == cudaSuccess)
-    err = cudaMemcpyAsync(&active, e->at<int>(L.o_scal), 4, cudaMemcpyDeviceToHost, e->stream);
+    err = cudaMemcpyAsync(e->readback, e->at<int>(L.o_scal), 4, cudaMemcpyDeviceToHost, e->stream);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(e->readback + 1, &e->at<WsHeader>(L.o_hdr)->status, 4,
+                          cudaMemcpyDeviceToHost, e->stream);
   if (err == cudaSuccess)
     err = cudaMemcpyAsync(e->done_h, e->at<int>(L.o_done), (size_t)L.slots * 4, cudaMemcpyDeviceToHost,
                           e->stream);
-  if (err == cudaSuccess)
-    err = cudaMemcpyAsync(&status, &e->at<WsHeader>(L.o_hdr)->status, 4, cudaMemcpyDeviceToHost, e->stream);
-  if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
   if (err != cudaSuccess) return fail_cuda(err);
+  e->launched = 1;
+  return LAKER_OK;
+}
+
+extern "C" int laker_engine_sync(void* host, int* running) {
+  EngineHost* e = engine_of(host);
+  if (!e || !running) return LAKER_ERR_INVALID_ARG;
+  if (!e->launched) {
+    *running = e->running;
+    return LAKER_OK;
+  }
+  cudaError_t err = cudaStreamSynchronize(e->stream);
+  e->launched = 0;
+  if (err != cudaSuccess) return fail_cuda(err);
+  const EngineLayout& L = e->L;
   for (int k = 0; k < L.slots; ++k)
     if (e->slots[k].state == kRunning && e->done_h[k]) e->slots[k].state = kStopped;
-  e->running = active;
-  *running = active;
-  return status ? status : LAKER_OK;
+  e->running = e->readback[0];
+  *running = e->running;
+  return e->readback[1] ? e->readback[1] : LAKER_OK;
+}
+
+extern "C" int laker_engine_step(void* host, int* running) {
+  const int st = laker_engine_launch(host);
+  if (st != LAKER_OK) return st;
+  return laker_engine_sync(host, running);
 }
 
 extern "C" int laker_engine_finished(void* host, int* slots, int max_slots, int* count) {
@@ -943,6 +970,7 @@ extern "C" int laker_engine_finished(void* host, int* slots, int max_slots, int*
 extern "C" int laker_engine_collect(void* host, int slot, double* x, laker_pcg_result* res) {
   EngineHost* e = engine_of(host);
   if (!e || slot < 0 || slot >= e->cfg.max_slots || !x || !res) return LAKER_ERR_INVALID_ARG;
+  if (e->launched) return LAKER_ERR_INVALID_ARG;  // between replays only
   if (e->slots[slot].state != kStopped) return LAKER_ERR_INVALID_ARG;
   const EngineLayout& L = e->L;
   const SlotInfo& si = e->slots[slot].info;

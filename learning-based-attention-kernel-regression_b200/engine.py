@@ -84,7 +84,9 @@ class SolveEngine:
         if hbytes == 0 or wbytes == 0:
             raise ValueError("invalid engine configuration")
         self.stream = stream if stream is not None else torch.cuda.Stream(device=self.device)
-        self._host = ctypes.create_string_buffer(hbytes)
+        # pinned, so that launch() returns before the replay completes
+        self._host_buf = torch.empty(hbytes, dtype=torch.uint8, pin_memory=True)
+        self._host = ctypes.c_void_p(self._host_buf.data_ptr())
         self.workspace = torch.empty(wbytes, dtype=torch.uint8, device=self.device)
         self.workspace_bytes = wbytes
         self._lib = lib
@@ -126,6 +128,17 @@ class SolveEngine:
         """One graph replay (chunk iterations of every running instance)."""
         running = ctypes.c_int(0)
         _lib.check(self._lib.laker_engine_step(self._host, ctypes.byref(running)), "laker_engine_step")
+        self.running = running.value
+        return self.running
+
+    def launch(self) -> None:
+        """Start one graph replay without waiting (admit/collect wait for sync)."""
+        _lib.check(self._lib.laker_engine_launch(self._host), "laker_engine_launch")
+
+    def sync(self) -> int:
+        """Wait for the replay started by launch(); running instances after it."""
+        running = ctypes.c_int(0)
+        _lib.check(self._lib.laker_engine_sync(self._host, ctypes.byref(running)), "laker_engine_sync")
         self.running = running.value
         return self.running
 
