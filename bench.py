@@ -479,6 +479,294 @@ def count_reference_iterations(args) -> None:
                       rn / float(np.linalg.norm(y.numpy())), "true_relres": true_rel}))
 
 
+# ---------------------------------------------------------------------------
+# other workloads (one JSON line each; the default workload is the solve above)
+# ---------------------------------------------------------------------------
+def _peaks_file() -> dict:
+    try:
+        return json.loads((REPO / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        return {}
+
+
+def _event_ms(fn, reps: int = 3) -> float:
+    fn()
+    torch.cuda.synchronize()
+    out = []
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        out.append(a.elapsed_time(b))
+    return min(out)
+
+
+def _base_line(metric, value, unit, args, ms, dtype, config, higher=True):
+    return {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": higher, "scaling": "weak",
+            "vs_baseline": None, "dtype": dtype, "data": "synthetic", "config": config}
+
+
+def workload_fit(args) -> None:
+    """Config: n=2000 fit + predict at 2000 points through LAKERRegressor."""
+    import laker_b200 as L
+    from oracle import laker_oracle as O
+
+    dev = torch.device("cuda", 0)
+    n = 2000
+    x, y, xq = L.synthetic_field(n, 0, m=2000)
+
+    def step():
+        model = L.LAKERRegressor(embedding_dim=EMBED_DIM, lambda_reg=LAMBDA, gamma=0.1, pcg_tol=TOL,
+                                 pcg_max_iter=MAX_ITER, device=dev, dtype=torch.float32, verbose=False)
+        model.fit(x, y, seed=0)
+        pred = model.predict(xq)
+        torch.cuda.synchronize()
+        return model, pred
+
+    for _ in range(args.warmup):
+        step()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        model, pred = step()
+        times.append((time.perf_counter() - t0) * 1e3)
+    ms = float(statistics.median(times))
+    # float64 oracle with the same probes and FP32-computed embeddings
+    E = model.embeddings.double().cpu().numpy()
+    Eq = model.embedding_model(xq.to(dev)).detach().double().cpu().numpy()
+    probes = L.preconditioner.draw_probes(n, model.preconditioner.nr, torch.float32, dev, 0)
+    t0 = time.perf_counter()
+    alpha_o, iters_o, _ = O.fit(E, y.double().numpy(), lam=LAMBDA, probes=probes.double().cpu().numpy(),
+                                pcg_tol=TOL)
+    pred_o = O.predict(Eq, E, alpha_o)
+    cpu_s = time.perf_counter() - t0
+    line = _base_line("fits+predicts/sec (n=2000 fit, 2000 predictions)", 1e3 / ms, "fits/s", args, ms,
+                      "f32", {"workload": "LAKERRegressor.fit + predict, n=2000 train / 2000 test, d=10, "
+                              "lambda=1e-2, CCCP default N_r=200, tol 1e-6 (true float64 residual), seed 0",
+                              "n": n})
+    line["pcg_iterations"] = int(model.pcg_iterations_)
+    line["prediction_relerr_vs_float64_oracle"] = float(
+        np.linalg.norm(pred.double().cpu().numpy() - pred_o) / np.linalg.norm(pred_o))
+    line["relres_true"] = O.relres(E, LAMBDA, model.alpha.double().cpu().numpy(), y.double().numpy())
+    line["cpu_baseline"] = {"value": 1.0 / cpu_s, "unit": "fits/s", "cores": O.c_threads(), "kind": "port",
+                            "sample": f"float64 oracle fit + predict, full workload ({cpu_s:.2f} s, "
+                                      f"{iters_o} PCG iterations)"}
+    print(json.dumps(line), flush=True)
+
+
+def workload_variance(args) -> None:
+    """Config: n=20000, predictive variance at 512 query points (512 RHS)."""
+    import laker_b200 as L
+    from laker_b200 import _lib
+    from oracle import laker_oracle as O
+
+    dev = torch.device("cuda", 0)
+    n, m = 20000, 512
+    x, y, xq = L.synthetic_field(n, 0, m=m)
+    emb = L.PositionEmbedding(2, EMBED_DIM, device=dev, dtype=torch.float32)
+    with torch.no_grad():
+        E = emb(x.to(dev))
+    op = L.AttentionKernelOperator(E, lambda_reg=LAMBDA)
+    pre = L.CCCPPreconditioner(gamma=0.1, verbose=False, device=dev, dtype=torch.float32).build(
+        op.matvec, n, seed=0)
+    core = L.LAKERCore(embedding_dim=EMBED_DIM, pcg_tol=TOL, pcg_max_iter=MAX_ITER, device=dev,
+                       dtype=torch.float32, verbose=False)
+    xq_d = xq.to(dev)
+
+    def step():
+        return core.predict_variance(xq_d, emb, E, op, pre, None, LAMBDA)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    clocks.start()
+    for i in range(args.steps):
+        ev[i][0].record()
+        var = step()
+        ev[i][1].record()
+    torch.cuda.synchronize()
+    clocks.stop()
+    ms_steps = [a.elapsed_time(b) for a, b in ev]
+    ms = float(statistics.median(ms_steps))
+    pcg = core.last_pcg
+    # per-column sigma^2 on 8 columns against float64 solves of the same columns
+    # (FP64 operator and recurrence): at the same tolerance (the reference's
+    # algorithm in float64) and converged (tol 1e-10).  sigma^2 = k(q,q) -
+    # k_q^T A^-1 k_q cancels, so its relative error is the solve's error
+    # amplified by k(q,q) / sigma^2; the error against k(q,q) is also given.
+    Eq = emb(xq_d).detach()
+    cols = list(range(0, m, m // 8))[:8]
+    q64 = _lib.pack_f64(Eq[cols].double())
+    kxq = _lib.kernel_eval(op.packed.packed64, n, q64, len(cols), EMBED_DIM, 0, torch.float64, dev)
+    kqq = torch.exp((Eq[cols].double() ** 2).sum(dim=1))
+    errs = {}
+    for name, tol in (("same_tol_float64", TOL), ("converged_float64", 1e-10)):
+        ref = L.PreconditionedConjugateGradient(tol=tol, max_iter=5000, verbose=False)
+        v64 = ref._solve_generic(op.matvec_f64, pre.apply, kxq, None, 5000)
+        var64 = _lib.variance_finalize(q64, len(cols), EMBED_DIM, kxq, v64.to(torch.float64))
+        diff = (var[cols].double() - var64).abs()
+        errs[name] = {"max_relerr": (diff / var64.abs().clamp(min=1e-300)).max().item(),
+                      "max_err_over_kqq": (diff / kqq).max().item()}
+    # the dominant kernel: the tensor-core 512-RHS matvec alone
+    X = torch.randn(n, m, device=dev)
+    k2_ms = _event_ms(lambda: op.matvec(X))
+    tf32 = 3 * 2.0 * n * n * m / (k2_ms * 1e-3) / 1e12
+    pk = _peaks_file()
+    tf32_peak = pk.get("bf16_tflops", 1590.0) / 2.0
+    # CPU: one 512-RHS float64 matvec on a row sample, x iterations
+    import numpy as _np
+    Eh = E.double().cpu().numpy()
+    Xh = _np.random.default_rng(0).standard_normal((n, m))
+    rows = 256
+    t0 = time.perf_counter()
+    O.rect_matvec(Eh[:rows], Eh, Xh)
+    t_rows = time.perf_counter() - t0
+    t_iter = t_rows * n / rows
+    cpu_rate = m / (t_iter * max(pcg.iterations, 1))
+    line = _base_line("variance queries/sec (n=20k, 512 queries, 1e-6 resid)", m / (ms * 1e-3),
+                      "queries/s", args, ms, "f32",
+                      {"workload": f"LAKERCore.predict_variance, n={n} train, m={m} queries (512 RHS), "
+                                   "d=10, CCCP default N_r, tol 1e-6 (float64 residual, global Frobenius "
+                                   "norm as solve_2d)", "n": n, "m": m})
+    line.update({
+        "pcg_iterations": pcg.iterations, "fp64_residual_recomputations": pcg.accurate_matvecs,
+        "relres_frobenius": pcg.residual_norm / max(getattr(pcg, "rhs_norm", 0.0), 1e-300),
+        "variance_error_8_columns": errs,
+        "roofline": {"bound": "tensor", "kernel": "k2_tc_matvec (tcgen05 kind::tf32, 3 split products)",
+                     "achieved": tf32, "peak": tf32_peak, "unit": "TFLOP/s", "frac": tf32 / tf32_peak,
+                     "traffic": None, "avg_launch_ms": k2_ms,
+                     "peak_source": "half of the measured cuBLAS bf16 burst (MEASURED_PEAKS.json): TF32 "
+                                    "dense rate"},
+        "clocks": clocks.summary(),
+        "cpu_baseline": {"value": cpu_rate, "unit": "queries/s", "cores": O.c_threads(), "kind": "port",
+                         "sample": f"float64 oracle 512-RHS matvec on {rows} of {n} rows ({t_rows:.2f} s) "
+                                   f"scaled to one iteration x {pcg.iterations} iterations (extrapolated)"},
+    })
+    print(json.dumps(line), flush=True)
+
+
+def workload_batch(args) -> None:
+    """Config: 1024 independent regressions, n log-uniform in [500, 20000]."""
+    import laker_b200 as L
+    from oracle import laker_oracle as O
+
+    dev = torch.device("cuda", 0)
+    count = args.count
+    ns, lams = L.batch_instances(count)
+    ops, ys = [], []
+    emb = L.PositionEmbedding(2, EMBED_DIM, device=dev, dtype=torch.float32)
+    for i, (n, lam) in enumerate(zip(ns, lams)):
+        x, y, _ = L.synthetic_field(n, i)
+        with torch.no_grad():
+            E = emb(x.to(dev))
+        ops.append(L.AttentionKernelOperator(E, lambda_reg=lam))
+        ys.append(y.to(dev).double())
+    torch.cuda.synchronize()
+    tm = {}
+    t0 = time.perf_counter()
+    pres = L.build_cccp_batched(ops, seeds=list(range(count)), timings=tm)
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    pcg = L.BatchedPCG(tol=TOL, max_iter=MAX_ITER)
+    for _ in range(args.warmup):
+        pcg.solve(ops, pres, ys)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    times = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        xs = pcg.solve(ops, pres, ys)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    clocks.stop()
+    solve_s = float(statistics.median(times))
+    worst = 0.0
+    for k in range(0, count, max(1, count // 16)):
+        r = ops[k].residual_f64(xs[k], ys[k])
+        worst = max(worst, (torch.linalg.norm(r) / torch.linalg.norm(ys[k])).item())
+    # the plain single-instance path on an evenly spaced subset, scaled by count
+    sub = list(range(0, count, max(1, count // args.plain_subset)))[:args.plain_subset]
+    single = L.PreconditionedConjugateGradient(tol=TOL, max_iter=MAX_ITER, verbose=False)
+    t_plain = 0.0
+    for k in sub:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        single.solve(ops[k].matvec, pres[k].apply, ys[k])
+        torch.cuda.synchronize()
+        t_plain += time.perf_counter() - t0
+    plain_rate = len(sub) / t_plain
+    # CPU: float64 oracle iteration cost on a few instances, x their iterations
+    cpu_t = 0.0
+    csub = sub[: max(1, len(sub) // 8)]
+    for k in csub:
+        Eh = ops[k].embeddings.double().cpu().numpy()
+        v = np.random.default_rng(k).standard_normal(ops[k].n)
+        t0 = time.perf_counter()
+        O.attention_matvec(Eh, lams[k], v)
+        cpu_t += (time.perf_counter() - t0) * pcg.iterations[k]
+    cpu_rate = len(csub) / cpu_t
+    line = _base_line("batched PCG solves/sec (1024 uneven instances @1e-6 resid)", count / solve_s,
+                      "solves/s", args, solve_s * 1e3, "f32",
+                      {"workload": f"{count} independent regressions, n log-uniform in [500, 20000], "
+                                   "lambda log-uniform in [1e-3, 1e-1], d=10, CCCP default N_r per "
+                                   "instance (built beforehand, batched), tol 1e-6 true float64 residual",
+                       "instances": count, "total_points": int(sum(ns))})
+    line.update({
+        "iterations_max": max(pcg.iterations), "iterations_mean": sum(pcg.iterations) / count,
+        "worst_sampled_relres": worst, "statuses_ok": sum(1 for s in pcg.statuses if s == 0),
+        "batched_cccp_build_s": build_s, "build_phases_s": tm,
+        "plain_single_instance_solves_per_s": plain_rate,
+        "speedup_vs_plain": (count / solve_s) / plain_rate,
+        "gpu_launches": pcg.kernel_launches, "clocks": clocks.summary(),
+        "cpu_baseline": {"value": cpu_rate, "unit": "solves/s", "cores": O.c_threads(), "kind": "port",
+                         "sample": f"float64 oracle matvec of {len(csub)} instances x their iteration "
+                                   "counts (extrapolated)"},
+    })
+    print(json.dumps(line), flush=True)
+
+
+def workload_serve(args) -> None:
+    """Config: Poisson trace of fit (70 %) and variance (30 %) requests."""
+    import laker_b200  # noqa: F401
+    from laker_b200.serving import Server, make_trace, run_plain, summarize
+
+    dev = torch.device("cuda", 0)
+    rates = [float(r) for r in args.rates.split(",")]
+    out = []
+    for rate in rates:
+        trace = make_trace(args.requests, rate, seed=0, n_range=(1000, 50000), m_range=(16, 256))
+        srv = Server(device=dev, hbm_budget=150e9)
+        warm = make_trace(6, 1e4, seed=99, n_range=(1000, 4000), m_range=(16, 32))
+        srv.run(warm)
+        recs = srv.run(trace)
+        s = summarize(recs)
+        plain = run_plain(srv, trace)
+        p = summarize(plain)
+        out.append({"rate": rate, "served": s, "plain": p,
+                    "speedup_requests_per_s": s["requests_per_s"] / p["requests_per_s"]})
+        srv.engine.release()
+        del srv
+        torch.cuda.empty_cache()
+    best = out[-1]
+    line = _base_line("served requests/sec with p50/p99 latency (Poisson fit/variance trace)",
+                      best["served"]["requests_per_s"], "requests/s", args,
+                      best["served"]["makespan_s"] * 1e3, "f32",
+                      {"workload": f"{args.requests} requests per rate, Poisson arrivals, 70 % fit "
+                                   "(n log-uniform in [1000, 50000]) / 30 % variance (16-256 query "
+                                   "points) against a resident model, HBM budget 150 GB, tol 1e-6",
+                       "rates": rates})
+    line.update({"p50_ms": best["served"]["p50_ms"], "p99_ms": best["served"]["p99_ms"],
+                 "by_rate": out})
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawTextHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -492,7 +780,19 @@ def main() -> None:
     ap.add_argument("--count-reference-iterations", action="store_true")
     ap.add_argument("--kernel-only", action="store_true",
                     help="time the FP32 fused matvec alone (profiling target)")
+    ap.add_argument("--workload", choices=("solve", "fit", "variance", "batch", "serve"),
+                    default="solve", help="solve: n=100k PCG solve (the default line); fit: n=2000 "
+                    "fit+predict; variance: n=20k x 512 queries; batch: 1024 instances; serve: "
+                    "Poisson request trace")
+    ap.add_argument("--count", type=int, default=1024, help="batch: instances")
+    ap.add_argument("--plain-subset", type=int, default=64, help="batch: single-path sample")
+    ap.add_argument("--requests", type=int, default=120, help="serve: requests per rate")
+    ap.add_argument("--rates", default="100", help="serve: comma-separated arrival rates (req/s)")
     args = ap.parse_args()
+    if args.workload != "solve" and args.impl == "ours":
+        {"fit": workload_fit, "variance": workload_variance, "batch": workload_batch,
+         "serve": workload_serve}[args.workload](args)
+        return
     if args.warmup < 3 and args.impl == "ours" and not args.kernel_only:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     if args.kernel_only:

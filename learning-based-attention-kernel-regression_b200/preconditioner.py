@@ -191,10 +191,17 @@ class CCCPPreconditioner:
             iso_prev = iso
             qbm_prev = qbm.clone()
             m_mat = eye * iso + qbm
-            evals, evecs = eigh_stable(m_mat, eps=self.epsilon)
-            proj = evecs.T @ self.qr_r
-            inv_m_r = proj.T @ (evals.reciprocal().unsqueeze(-1) * proj)
-            denom = torch.diagonal(inv_m_r) + self.epsilon
+            # diag(R^T M^-1 R) by a Cholesky solve (M = c I + B is SPD); the
+            # reference forms it from eigh(M) (laker/preconditioner.py:207-225),
+            # which gives the same values at a few times the cost
+            chol, info = torch.linalg.cholesky_ex(m_mat)
+            if int(info.item()) == 0:
+                denom = (self.qr_r * torch.cholesky_solve(self.qr_r, chol)).sum(dim=0) + self.epsilon
+            else:
+                evals, evecs = eigh_stable(m_mat, eps=self.epsilon)
+                proj = evecs.T @ self.qr_r
+                inv_m_r = proj.T @ (evals.reciprocal().unsqueeze(-1) * proj)
+                denom = torch.diagonal(inv_m_r) + self.epsilon
             weights = (n / self.nr) / denom
             wrr = (self.qr_r * weights.unsqueeze(0)) @ self.qr_r.T
             f_gamma = (wrr + self.gamma * eye) * (1.0 / reg_scale)

@@ -147,6 +147,7 @@ class PreconditionedConjugateGradient:
         self.iterations = int(res.iterations)
         self.accurate_matvecs = int(res.accurate_matvecs)
         self.residual_norm = float(res.residual_norm)
+        self.rhs_norm = float(res.rhs_norm)
         self.recurrence_norm = float(res.recurrence_norm)
         self.status = int(res.status)
         if res.rhs_norm == 0.0:
@@ -165,6 +166,7 @@ class PreconditionedConjugateGradient:
             x = x0.to(device=b.device, dtype=torch.float64).clone()
             r = op.residual_f64(x, b)
         bn = torch.linalg.norm(b).item()
+        self.rhs_norm = bn
         self.accurate_matvecs = 0 if x0 is None else 1
         if bn == 0:
             self.iterations = 0
