@@ -434,7 +434,9 @@ def run_ours(args) -> None:
 
 
 def kernel_only(args) -> None:
-    """FP32 fused matvec alone on the bench embeddings (a clean ncu target)."""
+    """One fused matvec alone on the bench embeddings (a clean ncu target):
+    the FP32 single-RHS operator, or with --rhs k > 1 the tensor-core
+    multi-RHS operator."""
     import laker_b200 as L
 
     dev = torch.device("cuda", 0)
@@ -443,7 +445,7 @@ def kernel_only(args) -> None:
     with torch.no_grad():
         E = emb(x.to(dev))
     op = L.AttentionKernelOperator(E, lambda_reg=LAMBDA)
-    v = torch.randn(args.n, device=dev)
+    v = torch.randn(args.n, device=dev) if args.rhs <= 1 else torch.randn(args.n, args.rhs, device=dev)
     for _ in range(args.warmup):
         op.matvec(v)
     torch.cuda.synchronize()
@@ -454,8 +456,12 @@ def kernel_only(args) -> None:
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / max(args.steps, 1)
-    print(json.dumps({"kernel": "fp32 fused matvec", "n": args.n, "ms": ms,
-                      "entries_per_s": args.n * args.n / (ms * 1e-3)}))
+    k = max(args.rhs, 1)
+    out = {"kernel": "fp32 fused matvec" if k == 1 else "tensor-core multi-RHS matvec", "n": args.n,
+           "rhs": k, "ms": ms, "entries_per_s": args.n * args.n / (ms * 1e-3)}
+    if k > 1:
+        out["tf32_tflops_3_products"] = 3 * 2.0 * args.n * args.n * k / (ms * 1e-3) / 1e12
+    print(json.dumps(out))
 
 
 def count_reference_iterations(args) -> None:
@@ -784,6 +790,7 @@ def main() -> None:
                     default="solve", help="solve: n=100k PCG solve (the default line); fit: n=2000 "
                     "fit+predict; variance: n=20k x 512 queries; batch: 1024 instances; serve: "
                     "Poisson request trace")
+    ap.add_argument("--rhs", type=int, default=1, help="--kernel-only: right-hand sides")
     ap.add_argument("--count", type=int, default=1024, help="batch: instances")
     ap.add_argument("--plain-subset", type=int, default=64, help="batch: single-path sample")
     ap.add_argument("--requests", type=int, default=120, help="serve: requests per rate")
