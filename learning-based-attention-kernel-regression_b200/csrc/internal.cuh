@@ -55,7 +55,7 @@ cudaError_t launch_multi_f64(const double* rows64, int64_t m, const double* cols
 
 // Tensor-core (tcgen05, split TF32) multi-RHS FP32 matvec (matvec_tc.cu).
 int k2_chunk_cols(int k);
-size_t k2_image_bytes(int64_t n, int k);
+size_t k2_image_bytes(int64_t m, int64_t n, int k);
 bool k2_use_tensor_cores();
 cudaError_t launch_k2(const float* rows32, int64_t m, const float* cols32, int64_t n, int d,
                       int clamp, float lam, const float* X, int64_t ldx, int k, float* Y,

@@ -450,7 +450,7 @@ extern "C" size_t laker_matvec_workspace_bytes(int64_t m, int64_t n, int d, int 
   if (m < 0 || n < 0 || d < 1 || d > 16 || k < 1) return 0;
   if (k > 1) {
     // the tensor-core path stages X as split, swizzled TF32 tiles
-    return kWsHeader + (k2_use_tensor_cores() && n > 0 ? (size_t)round_up((int64_t)k2_image_bytes(n, k), 256) : 0);
+    return kWsHeader + (k2_use_tensor_cores() && n > 0 ? (size_t)round_up((int64_t)k2_image_bytes(m, n, k), 256) : 0);
   }
   const SegPlan p = precision == 64 ? k4_plan(m, n, d) : k1_plan(m, n, d);
   size_t bytes = (size_t)p.S * (size_t)m * sizeof(double);
