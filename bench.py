@@ -753,6 +753,7 @@ def workload_serve(args) -> None:
         srv.run(warm)
         recs = srv.run(trace)
         s = summarize(recs)
+        s["activity_s"] = dict(srv.stats)
         plain = run_plain(srv, trace)
         p = summarize(plain)
         out.append({"rate": rate, "served": s, "plain": p,

@@ -20,14 +20,13 @@ from __future__ import annotations
 
 import ctypes
 import logging
-import time
 from typing import List, Optional, Sequence
 
 import torch
 
 from . import _lib
 from .kernels import AttentionKernelOperator
-from .preconditioner import (CCCPPreconditioner, adaptive_shrinkage_rho, draw_probes,
+from .preconditioner import (CCCPPreconditioner, PhaseClock, adaptive_shrinkage_rho, draw_probes,
                              inv_sqrt_spd_batched, orthonormal_basis)
 
 logger = logging.getLogger(__name__)
@@ -57,7 +56,7 @@ def build_cccp_batched(
         return []
     dev = operators[0].device
     f64 = torch.float64
-    clock = _PhaseClock(timings, dev)
+    clock = PhaseClock(timings, dev)
     pres, rs, ns, nrs = [], [], [], []
     for k, op in enumerate(operators):
         n = op.n
@@ -145,25 +144,6 @@ def build_cccp_batched(
         pre._prepare_apply(W[k, :nr, :nr])
     clock.stop("apply_factors")
     return pres
-
-
-class _PhaseClock:
-    """Accumulates synchronised wall time per phase into a dict (or nothing)."""
-
-    def __init__(self, out: Optional[dict], device: torch.device) -> None:
-        self.out, self.device, self.t = out, device, 0.0
-
-    def start(self) -> None:
-        if self.out is not None:
-            torch.cuda.synchronize(self.device)
-            self.t = time.perf_counter()
-
-    def stop(self, phase: str) -> None:
-        if self.out is not None:
-            torch.cuda.synchronize(self.device)
-            now = time.perf_counter()
-            self.out[phase] = self.out.get(phase, 0.0) + now - self.t
-            self.t = now
 
 
 class BatchedPCG:

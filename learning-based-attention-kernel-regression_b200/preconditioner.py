@@ -19,6 +19,7 @@ reproduces a reference build run on the CPU (the float64 goldens).
 from __future__ import annotations
 
 import logging
+import time
 from typing import Callable, Optional
 
 import torch
@@ -27,6 +28,25 @@ from . import _lib
 from .backend import get_default_device, get_default_dtype
 
 logger = logging.getLogger(__name__)
+
+
+class PhaseClock:
+    """Accumulates synchronised wall time per phase into a dict (or nothing)."""
+
+    def __init__(self, out: Optional[dict], device: torch.device) -> None:
+        self.out, self.device, self.t = out, device, 0.0
+
+    def start(self) -> None:
+        if self.out is not None:
+            torch.cuda.synchronize(self.device)
+            self.t = time.perf_counter()
+
+    def stop(self, phase: str) -> None:
+        if self.out is not None:
+            torch.cuda.synchronize(self.device)
+            now = time.perf_counter()
+            self.out[phase] = self.out.get(phase, 0.0) + now - self.t
+            self.t = now
 
 
 def adaptive_shrinkage_rho(num_probes: int, problem_size: int, gamma: float,
@@ -149,8 +169,12 @@ class CCCPPreconditioner:
 
     # ------------------------------------------------------------------
     def build(self, operator: Callable[[torch.Tensor], torch.Tensor], n: int,
-              seed: Optional[int] = None) -> "CCCPPreconditioner":
-        """Learn the preconditioner (laker/preconditioner.py:144-284)."""
+              seed: Optional[int] = None, timings: Optional[dict] = None) -> "CCCPPreconditioner":
+        """Learn the preconditioner (laker/preconditioner.py:144-284).
+
+        `timings`, when given, receives the seconds spent in each phase
+        (probes, operator, qr, fixed_point, apply_factors) and the fixed
+        point's iteration count under "iterations"."""
         if self.device.type != "cuda":
             raise RuntimeError("CCCPPreconditioner on the B200 path requires a CUDA device")
         dev, dt = self.device, self.dtype
@@ -162,7 +186,10 @@ class CCCPPreconditioner:
         if self.verbose:
             logger.info("Building CCCP preconditioner: n=%d, N_r=%d", n, self.nr)
 
+        clock = PhaseClock(timings, dev)
+        clock.start()
         probes = draw_probes(n, self.nr, dt, self.probe_device, seed).to(dev)
+        clock.stop("probes")
 
         if self.probe_strategy == "power_iter":
             n_power = max(1, int(self.nr * 0.25))
@@ -175,11 +202,13 @@ class CCCPPreconditioner:
         # operator(probes) through the fused multi-RHS kernel; QR and the
         # N_r x N_r fixed point then run in float64 on the GPU
         op_probes = operator(probes).to(torch.float64)
+        clock.stop("operator")
         dt = torch.float64
         norms = torch.linalg.norm(op_probes, dim=0, keepdim=True)
         normalized = op_probes / norms.clamp(min=self.epsilon)
         q_basis, qr_r = orthonormal_basis(normalized)
         self.q_basis, self.qr_r = q_basis, qr_r
+        clock.stop("qr")
 
         shrinkage = adaptive_shrinkage_rho(self.nr, n, self.gamma, self.base_rho)
         reg_scale = 1.0 + self.gamma / n
@@ -222,8 +251,12 @@ class CCCPPreconditioner:
         self.cccp_iterations = it + 1
         self.isotropic_coef = iso
         self.q_basis_matrix = qbm
+        clock.stop("fixed_point")
+        if timings is not None:
+            timings["iterations"] = timings.get("iterations", 0) + it + 1
         self.q_eigenvalues, self.q_eigenvectors = eigh_stable(eye * iso + qbm, eps=self.epsilon)
         self._prepare_apply()
+        clock.stop("apply_factors")
         if self.verbose:
             logger.info("CCCP preconditioner built in %d iterations", it + 1)
         return self

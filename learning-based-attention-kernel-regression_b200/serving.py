@@ -161,6 +161,9 @@ class Server:
         self.core = LAKERCore(embedding_dim=embedding_dim, pcg_tol=tol, pcg_max_iter=max_iter,
                               device=self.device, dtype=torch.float32, verbose=False)
         self.outputs: Dict[int, torch.Tensor] = {}
+        # wall seconds of the last run by activity: fit preparation and
+        # engine waits (main thread), variance solves (worker), idle waits
+        self.stats: Dict[str, float] = {}
 
     # ------------------------------------------------------------------
     def _nr(self, n: int) -> int:
@@ -211,6 +214,12 @@ class Server:
             return clock() if realtime else fake_now[0]
 
         errors: List[BaseException] = []
+        # set by the worker after every variance request it ends: the main
+        # loop waits on it instead of spinning (a spinning loop holds the GIL
+        # and starves the worker)
+        wake = threading.Event()
+        stats = self.stats = {"prepare_s": 0.0, "engine_wait_s": 0.0, "variance_s": 0.0,
+                              "idle_s": 0.0, "replays": 0}
 
         def worker():
             try:
@@ -226,9 +235,12 @@ class Server:
                         if model is None or model.alpha is None:  # its fit failed
                             rec.status = _lib.LAKER_ERR_CAPACITY
                             rec.finish = now()
+                            wake.set()
                             continue
+                        tv = time.perf_counter()
                         var = self.variance(model, req)
                         self.var_stream.synchronize()
+                        stats["variance_s"] += time.perf_counter() - tv
                         rec.finish = now()
                         pcg = self.core.last_pcg
                         rec.iterations = pcg.iterations if pcg is not None else 0
@@ -237,8 +249,10 @@ class Server:
                         with lock:
                             var_outstanding[req.target] -= 1
                             model.last_use = now()
+                        wake.set()
             except BaseException as ex:  # surfaced by the main loop
                 errors.append(ex)
+                wake.set()
 
         th = threading.Thread(target=worker, daemon=True)
         th.start()
@@ -265,7 +279,9 @@ class Server:
                 if errors:
                     raise errors[0]
                 t = now()
+                progress = False
                 while pending and pending[0].arrival <= t:
+                    progress = True
                     r = pending.popleft()
                     if r.kind == "fit":
                         fit_queue.append(r)
@@ -297,18 +313,26 @@ class Server:
                         records[r.rid].status = _lib.LAKER_ERR_CAPACITY
                         records[r.rid].finish = now()
                         release_variance(r.rid)
+                        progress = True
                     elif evict(need):
+                        progress = True
                         fit_queue.popleft()
                         with lock:
                             used[0] += need
                         if not r.refit:
                             records[r.rid].start = now()
+                        tp = time.perf_counter()
                         with torch.cuda.stream(self.build_stream):
                             model = self.prepare_fit(r)
+                        stats["prepare_s"] += time.perf_counter() - tp
                         ready.append((r, model))
                 if launched:
+                    tw = time.perf_counter()
                     eng.sync()
+                    stats["engine_wait_s"] += time.perf_counter() - tw
+                    stats["replays"] += 1
                 for slot in eng.finished():
+                    progress = True
                     x, res = eng.collect(slot)
                     r, model = inflight.pop(slot)
                     model.alpha = x
@@ -334,17 +358,23 @@ class Server:
                         break
                     ready.popleft()
                     inflight[slot] = (r, model)
+                    progress = True
                 # variance completions
                 done = sum(1 for rec in records.values() if not math.isnan(rec.finish))
-                if eng.running == 0 and not ready and not fit_queue:
-                    if pending and var_q.empty():
-                        wait = pending[0].arrival - now()
-                        if realtime and wait > 0:
-                            time.sleep(min(wait, 0.005))
-                        elif not realtime:
-                            fake_now[0] = max(fake_now[0], pending[0].arrival)
-                    else:
-                        time.sleep(0.0005)
+                if progress or launched or done >= total:
+                    continue
+                # nothing can move until a variance request ends, a request
+                # arrives or (without a real clock) time is advanced
+                if not realtime and pending and var_q.empty() and not ready and not fit_queue:
+                    fake_now[0] = max(fake_now[0], pending[0].arrival)
+                    continue
+                timeout = 0.05
+                if realtime and pending:
+                    timeout = min(timeout, max(pending[0].arrival - now(), 0.0))
+                ti = time.perf_counter()
+                wake.wait(timeout)
+                wake.clear()
+                stats["idle_s"] += time.perf_counter() - ti
         finally:
             var_q.put(None)
             th.join(timeout=600)
