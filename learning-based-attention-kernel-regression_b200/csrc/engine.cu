@@ -513,7 +513,9 @@ __global__ void __launch_bounds__(kCompactThreads)
 struct EngineLayout {
   int64_t cap_points = 0, cap_blocks = 0, cap_pairs = 0;
   int slots = 0, ustride = 4, dp = 2;
+  bool tc = false;  // FP32 operator on the tensor cores (operand image arena)
   size_t bytes = 0;
+  size_t o_img = 0;
   size_t o_hdr, o_slots, o_st, o_done, o_ctr, o_scal, o_acti, o_actp, o_needi, o_needp, o_vvec,
       o_binst, o_bpart, o_upart, o_p32, o_p64, o_b, o_x, o_r, o_z, o_p, o_ap, o_row32, o_col32,
       o_row64, o_col64;
@@ -561,6 +563,8 @@ EngineLayout engine_layout(const laker_engine_config& cfg) {
   L.o_col32 = take(PP * 4);
   L.o_row64 = take(PP * 8);
   L.o_col64 = take(PP * 8);
+  L.tc = k1t_enabled(cfg.d);
+  if (L.tc) L.o_img = take(k1t_image_bytes(L.cap_points));
   L.bytes = o;
   return L;
 }
@@ -630,8 +634,11 @@ cudaError_t engine_iteration(EngineHost* e, cudaStream_t cs) {
   double* col64 = e->at<double>(L.o_col64);
   int* status = &e->at<WsHeader>(L.o_hdr)->status;
   int* scal = e->at<int>(L.o_scal);
-  cudaError_t err = launch_k1s_batched(e->at<float>(L.o_p32), d, clamp, p, row32, col32, e->sp32,
-                                       e->bm32, status, ed.active, cs);
+  cudaError_t err =
+      L.tc ? launch_k1t_batched(e->at<uint8_t>(L.o_img), clamp, p, row32, col32, e->sp32, e->bm32,
+                                status, ed.active, cs)
+           : launch_k1s_batched(e->at<float>(L.o_p32), d, clamp, p, row32, col32, e->sp32, e->bm32,
+                                status, ed.active, cs);
   if (err != cudaSuccess) return err;
   eng_after_matvec_kernel<<<G, BT, 0, cs>>>(ed, e->sp32, e->bm32, row32, col32, p, Ap);
   eng_update_xr_kernel<<<G, BT, 0, cs>>>(ed, p, Ap, X, r);
@@ -661,6 +668,16 @@ cudaError_t move_down(char* dst, const char* src, size_t bytes, cudaStream_t s) 
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
+}
+
+// Operand image of a slot's points for the tensor-core FP32 kernel, from its
+// packed FP32 embeddings in the arena.
+cudaError_t pack_slot_image(EngineHost* e, const SlotInfo& si) {
+  const EngineLayout& L = e->L;
+  if (!L.tc) return cudaSuccess;
+  return launch_k1t_pack(e->at<float>(L.o_p32) + (size_t)si.seg * L.dp, si.npts, e->cfg.d,
+                         e->at<uint8_t>(L.o_img) + (size_t)si.blk_start * k1t_image_bytes(1),
+                         si.nblk * RB, e->stream);
 }
 
 // Re-places a slot's record and block map (device) from its host record.
@@ -707,6 +724,7 @@ cudaError_t compact_arenas(EngineHost* e) {
       mv(L.o_p, 4);
       si.blk_start = nb;
       si.seg = to;
+      if (err == cudaSuccess) err = pack_slot_image(e, si);
     }
     si.pair_start = np;
     nb += si.nblk;
@@ -772,7 +790,8 @@ extern "C" int laker_engine_init(void* host, size_t host_bytes, void* workspace,
   char* tail = static_cast<char*>(host) + round_up((int64_t)sizeof(EngineHost), 64);
   e->slots = reinterpret_cast<SlotHost*>(tail);
   e->done_h = reinterpret_cast<int*>(tail + (size_t)cfg->max_slots * sizeof(SlotHost));
-  e->sp32 = k1s_plan_pairs(L.cap_blocks, L.cap_pairs, cfg->d);
+  e->sp32 = L.tc ? k1t_plan_pairs(L.cap_blocks, L.cap_pairs)
+                 : k1s_plan_pairs(L.cap_blocks, L.cap_pairs, cfg->d);
   e->sp64 = k4s_plan_pairs(L.cap_blocks, L.cap_pairs, cfg->d);
   e->block_grid = (int)std::max<int64_t>(1, std::min<int64_t>(L.cap_blocks, 4 * (int64_t)sm_count()));
 
@@ -890,6 +909,7 @@ extern "C" int laker_engine_admit(void* host, int64_t n, double lambda_reg, cons
                           cudaMemcpyDeviceToDevice, s);
   if (err == cudaSuccess)
     err = cudaMemcpyAsync(e->at<double>(L.o_b) + info.seg, b, (size_t)n * 8, cudaMemcpyDeviceToDevice, s);
+  if (err == cudaSuccess) err = pack_slot_image(e, info);
   if (err == cudaSuccess) err = place_slot(e, k, true);
   if (err == cudaSuccess) {
     const EngineDev& ed = e->ed;

@@ -456,8 +456,10 @@ extern "C" size_t laker_matvec_workspace_bytes(int64_t m, int64_t n, int d, int 
   size_t bytes = (size_t)p.S * (size_t)m * sizeof(double);
   if (m == n && n > 0) {
     // a square product with the same embeddings may take the symmetric kernel
-    const size_t sym = precision == 64 ? sym_partial_bytes<double>(k4s_plan(n, d))
-                                       : sym_partial_bytes<float>(k1s_plan(n, d));
+    size_t sym = precision == 64 ? sym_partial_bytes<double>(k4s_plan(n, d))
+                                 : sym_partial_bytes<float>(k1s_plan(n, d));
+    if (precision != 64 && k1t_enabled(d))  // + the tensor-core kernel's operand image
+      sym = (size_t)round_up((int64_t)sym, 1024) + k1t_image_bytes(n);
     if (sym > bytes) bytes = sym;
   }
   return kWsHeader + bytes;
@@ -491,10 +493,18 @@ extern "C" int laker_attn_matvec_f32(const float* rows32, int64_t m, const float
   char* wbase = static_cast<char*>(workspace) + kWsHeader;
   if (rows32 == cols32 && m == n && k1_use_symmetric()) {
     // the operator itself: every off-diagonal entry evaluated once
-    const SymPlan sp = k1s_plan(n, d);
+    const bool tc = k1t_enabled(d);
+    const SymPlan sp = tc ? k1t_plan(n) : k1s_plan(n, d);
     double* rowpart = reinterpret_cast<double*>(wbase);
     float* colpart = sym_colpart_ptr<float>(wbase, sp);
-    e = launch_k1s(cols32, n, d, clamp, X, rowpart, colpart, sp, &hdr->status, nullptr, s);
+    if (tc) {
+      uint8_t* img = reinterpret_cast<uint8_t*>(wbase) + round_up((int64_t)sym_partial_bytes<float>(sp), 1024);
+      e = launch_k1t_pack(cols32, n, d, img, sp.nb * sym_block_points(), s);
+      if (e == cudaSuccess)
+        e = launch_k1t(img, n, clamp, X, rowpart, colpart, sp, &hdr->status, nullptr, s);
+    } else {
+      e = launch_k1s(cols32, n, d, clamp, X, rowpart, colpart, sp, &hdr->status, nullptr, s);
+    }
     if (e == cudaSuccess) e = launch_sym_finish(sp, rowpart, colpart, n, lam, X, Y, ldy, s);
     return e == cudaSuccess ? LAKER_OK : fail_cuda(e);
   }

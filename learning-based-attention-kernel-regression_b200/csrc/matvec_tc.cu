@@ -30,6 +30,7 @@
 #include <cstdlib>
 
 #include "internal.cuh"
+#include "tc.cuh"
 
 namespace laker {
 namespace {
@@ -56,81 +57,14 @@ struct TileCfg {
   }
 };
 
-// ---- tcgen05 / descriptor helpers -------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-// Shared-memory matrix descriptor for a K-major operand in a swizzled
-// canonical layout: rows of TK TF32, 8-row core groups SBO bytes apart, tiles
-// 1024-byte aligned.  The K step inside the row advances the start address
-// by 32 bytes per 8 TF32.
+// K-major operand descriptor of a TK-point tile.
 template <int TK>
 __device__ __forceinline__ uint64_t kmajor_desc(uint32_t saddr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);                  // start address [0,14)
-  d |= (uint64_t)1u << 16;                                   // LBO (unused when swizzled) [16,30)
-  d |= (uint64_t)(TileCfg<TK>::kSBO >> 4) << 32;             // SBO [32,46)
-  d |= (uint64_t)1u << 46;                                   // descriptor version (Blackwell) [46,48)
-  d |= (uint64_t)TileCfg<TK>::kLayout << 61;                 // swizzle mode [61,64)
-  return d;
+  return kmajor_desc_raw(saddr, TileCfg<TK>::kSBO, TileCfg<TK>::kLayout);
 }
 
 // Instruction descriptor: kind::tf32, D = FP32, A and B TF32 K-major, M = 128.
-__host__ __device__ constexpr uint32_t tf32_idesc(int n) {
-  return (1u << 4)                      // D format F32
-         | (2u << 7)                    // A format TF32
-         | (2u << 10)                   // B format TF32
-         | ((uint32_t)(n >> 3) << 17)   // N >> 3
-         | ((uint32_t)(kTcRows >> 4) << 24);  // M >> 4
-}
-
-__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
-                                         uint32_t idesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n"
-      :
-      : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-               :
-               : "r"(smem_u32(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ void fence_async_smem() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-
-__device__ __forceinline__ uint32_t to_tf32(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return r;
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
-      "%12, %13, %14, %15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
+__host__ __device__ constexpr uint32_t tf32_idesc(int n) { return tf32_idesc_mn(kTcRows, n); }
 
 // ---- X -> split, swizzled B tiles ---------------------------------------------
 // Image of chunk c (N right-hand sides), column tile t: [hi: N rows x 4 TK B]
@@ -190,28 +124,6 @@ struct K2Work {
   int64_t items;    // rtiles * chunks * segs
 };
 
-// Wait for a phase, giving up on timeout (sets *abort) or when another role
-// has set *abort.
-__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, int* status,
-                                              volatile int* abort) {
-  if (mbar_try_wait(bar, parity)) return true;
-  const uint64_t t0 = global_timer_ns();
-  for (uint32_t it = 0; it < (1u << 30); ++it) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if ((it & 63u) == 0) {
-      if (*abort) return false;
-      if (global_timer_ns() - t0 > 2000000000ull) break;
-    }
-  }
-  record_status(status, LAKER_ERR_TIMEOUT);
-  *abort = 1;
-  return false;
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
 template <int DP, bool CLAMP, int TK>
 __global__ void __launch_bounds__(kTcThreadsWs, 1)
     k2_tc_matvec(const float* __restrict__ rows32, int64_t m, const float* __restrict__ cols32,
@@ -248,13 +160,15 @@ __global__ void __launch_bounds__(kTcThreadsWs, 1)
       mbar_init(&b_full[i], 1);
       mbar_init(&b_empty[i], 1);
     }
+    // one arrival per entry warp (not per thread: arrivals on one mbarrier
+    // serialise)
     for (int i = 0; i < kASlots; ++i) {
-      mbar_init(&a_full[i], kEntryThreads);
+      mbar_init(&a_full[i], kEntryThreads / 32);
       mbar_init(&a_empty[i], 1);
     }
     for (int i = 0; i < 2; ++i) {
       mbar_init(&acc_full[i], 1);
-      mbar_init(&acc_empty[i], kEntryThreads);
+      mbar_init(&acc_empty[i], kEntryThreads / 32);
     }
     *abort = 0;
     mbar_fence_init();
@@ -400,8 +314,9 @@ __global__ void __launch_bounds__(kTcThreadsWs, 1)
           *reinterpret_cast<uint4*>(a_hi + off) = hi;
           *reinterpret_cast<uint4*>(a_lo + off) = lo;
         }
-        fence_async_smem();
-        mbar_arrive(&a_full[as]);
+        fence_async_smem();  // this thread's entries -> visible to the tensor core
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&a_full[as]);
       }
       if (!ok) break;
       // epilogue: this item's accumulators
@@ -430,7 +345,8 @@ __global__ void __launch_bounds__(kTcThreadsWs, 1)
         }
       }
       tc_fence_before();
-      mbar_arrive(&acc_empty[ab]);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[ab]);
     }
   }
 

@@ -304,6 +304,7 @@ struct PcgWs {
   double* blockpart;
   double* upart;
   double* v;
+  uint8_t* img;  // operand image of the tensor-core symmetric kernel (or null)
   size_t bytes;
 };
 
@@ -340,6 +341,7 @@ PcgWs carve(void* base, int64_t n, int d, int nr) {
   (void)nr;  // the apply's partials are sized for the largest padded row (1024)
   w.upart = reinterpret_cast<double*>(take((size_t)precond_grid() * kMaxNr * sizeof(double)));
   w.v = reinterpret_cast<double*>(take((size_t)kMaxNr * sizeof(double)));
+  w.img = k1t_enabled(d) ? reinterpret_cast<uint8_t*>(take(k1t_image_bytes(n))) : nullptr;
   w.bytes = off;
   return w;
 }
@@ -372,7 +374,8 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
   PcgWs w = carve(workspace, n, d, nr);
   const SegPlan p1 = k1_plan(n, n, d), p4 = k4_plan(n, n, d);
   const bool sym = k1_use_symmetric();
-  const SymPlan sp = k1s_plan(n, d);
+  const bool tc = sym && k1t_enabled(d);
+  const SymPlan sp = tc ? k1t_plan(n) : k1s_plan(n, d);
   double* sym_row = w.part32;
   float* sym_col = sym_colpart_ptr<float>(w.part32, sp);
   const int G = vec_grid(n), Gp = precond_grid();
@@ -409,9 +412,10 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
   h.active = 1;
   cudaError_t e = cudaMemsetAsync(w.hdr, 0, kWsHeader, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(w.st, &h, sizeof(PcgState), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && tc) e = launch_k1t_pack(op->packed32, n, d, w.img, sp.nb * sp.B, s);
   if (e != cudaSuccess) return fail_cuda(e);
 
-  int launches = 0;
+  int launches = tc ? 1 : 0;
   LaunchTimer t32, t64;
   t32.init(prm->profile != 0);
   t64.init(prm->profile != 0);
@@ -473,7 +477,9 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
     const int chunk = (prm->max_iter - launched) < check ? (prm->max_iter - launched) : check;
     for (int c = 0; c < chunk; ++c) {
       t32.begin(s);
-      if (sym) {
+      if (tc) {
+        launch_k1t(w.img, n, op->clamp, w.p, sym_row, sym_col, sp, dstatus, &w.st->active, s);
+      } else if (sym) {
         launch_k1s(op->packed32, n, d, op->clamp, w.p, sym_row, sym_col, sp, dstatus,
                    &w.st->active, s);
       } else {

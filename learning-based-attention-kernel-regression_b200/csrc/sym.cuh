@@ -115,6 +115,24 @@ cudaError_t launch_k1s(const float* E32, int64_t n, int d, int clamp, const floa
 cudaError_t launch_k1s_batched(const float* E32, int d, int clamp, const float* x,
                                double* rowpart, float* colpart, const SymPlan& sp,
                                const BatchMap& bm, int* status, const int* gate, cudaStream_t s);
+// Tensor-core symmetric FP32 kernel (matvec_symtc.cu): same blocks, pair
+// slots and partial layout as k1s, logits by tcgen05 split-TF32 MMAs from an
+// operand image of k1t_image_bytes(points) bytes (128 KB per 512 points,
+// indexed by point: an instance at seg uses blocks seg / 512 ...).
+bool k1t_enabled(int d);
+size_t k1t_image_bytes(int64_t points);
+SymPlan k1t_plan(int64_t n);
+SymPlan k1t_plan_pairs(int64_t nb, int64_t npairs);
+// image of `rows` points (a multiple of 512) from the packed FP32 layout;
+// points at or past npts are zero
+cudaError_t launch_k1t_pack(const float* packed32, int64_t npts, int d, uint8_t* img, int64_t rows,
+                            cudaStream_t s);
+cudaError_t launch_k1t(const uint8_t* img, int64_t n, int clamp, const float* x, double* rowpart,
+                       float* colpart, const SymPlan& sp, int* status, const int* gate,
+                       cudaStream_t s);
+cudaError_t launch_k1t_batched(const uint8_t* img, int clamp, const float* x, double* rowpart,
+                               float* colpart, const SymPlan& sp, const BatchMap& bm, int* status,
+                               const int* gate, cudaStream_t s);
 // y = lam x + (sum of the partials) for the standalone matvec.
 cudaError_t launch_sym_finish(const SymPlan& sp, const double* rowpart, const float* colpart,
                               int64_t n, float lam, const float* x, float* y, int64_t ldy,

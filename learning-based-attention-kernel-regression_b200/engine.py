@@ -39,12 +39,14 @@ def instance_blocks(n: int) -> Tuple[int, int]:
 
 
 def engine_bytes_per_instance(n: int, d: int, nr: int = 0) -> int:
-    """Device bytes an instance needs inside an engine sized for it alone."""
+    """Device bytes an instance needs inside an engine sized for it alone
+    (packed embeddings, vectors, the tensor-core operand image of 256 bytes
+    per point, pair partials, block partials)."""
     nb, npairs = instance_blocks(n)
     dp = (d + 1) // 2 * 2
     pts = nb * BLOCK
     ldq = max(4, (nr + 3) // 4 * 4)
-    return (pts * (12 * dp + 36) + npairs * BLOCK * 28 + nb * (32 + 4 * ldq + 4) + 4 * ldq + 512)
+    return (pts * (12 * dp + 36 + 256) + npairs * BLOCK * 28 + nb * (32 + 4 * ldq + 4) + 4 * ldq + 512)
 
 
 class SolveEngine:

@@ -59,6 +59,29 @@ def test_matvec_ragged_sizes(cuda, n):
     assert rel(op32.matvec(torch.tensor(x, device=cuda, dtype=torch.float32)), ref32) < F32_RTOL
 
 
+@pytest.mark.parametrize("n", [20000, 36100])
+def test_symmetric_operator_many_pairs_per_cta(cuda, n):
+    """The operator at sizes where every CTA of the persistent symmetric kernel
+    walks several block pairs (row-block changes, operand-stage reuse,
+    accumulator-buffer wrap-around; n = 20000: 820 pairs, 36100: 2485 pairs
+    over 148 CTAs), a partial last block, and repeated calls bit for bit."""
+    from laker_b200 import AttentionKernelOperator
+
+    rng = np.random.default_rng(n)
+    E = (rng.standard_normal((n, 10)) * 0.5).astype(np.float32)
+    x = rng.standard_normal(n)
+    ref = O.attention_matvec(E, 0.01, x)
+    op32 = AttentionKernelOperator(torch.tensor(E, device=cuda), lambda_reg=0.01)
+    xd = torch.tensor(x, device=cuda, dtype=torch.float32)
+    y1 = op32.matvec(xd)
+    y2 = op32.matvec(xd)
+    assert torch.equal(y1, y2)
+    assert rel(y1, ref) < F32_RTOL
+    # per-row agreement, not only in norm
+    err = np.abs(y1.cpu().double().numpy() - ref) / np.maximum(np.abs(ref), 1e-3 * np.abs(ref).max())
+    assert err.max() < 1e-4
+
+
 @pytest.mark.parametrize("d", [1, 2, 3, 5, 8, 11, 16])
 def test_matvec_all_dims(cuda, d):
     from laker_b200 import AttentionKernelOperator
