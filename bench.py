@@ -140,9 +140,11 @@ class ClockSampler:
         }
 
 
-def ncu_traffic_per_launch(n: int):
-    """DRAM bytes per FP32 matvec launch from the committed ncu summary, if any."""
-    path = REPO / "profiles" / "k1_matvec_f32_n100000.md"
+def ncu_traffic_per_launch(n: int, kernel_id: int = 1):
+    """DRAM bytes per FP32 operator launch from the committed ncu summary of
+    that kernel, if any."""
+    name = "k1t_matvec_n100000.md" if kernel_id == 2 else "k1_matvec_f32_n100000.md"
+    path = REPO / "profiles" / name
     if not path.exists():
         return None
     m = re.search(r"traffic_bytes_per_launch_n%d:\s*([0-9.eE+]+)" % n, path.read_text())
@@ -362,11 +364,13 @@ def run_ours(args) -> None:
         value = solves / (total_ms / 1e3)
         k1_avg_ms = k1_ms / max(k1_count, 1)
         # algorithmic work of the FP32 operator as the library evaluates it
-        # (symmetric kernel: each off-diagonal entry once, d + 2 FMA)
+        # (symmetric kernel: each off-diagonal entry once and used twice)
         work = _lib.fp32_matvec_work(n, EMBED_DIM)
+        kernel_id = _lib.fp32_operator_kernel(EMBED_DIM)
         flops_per_launch = work["flops"]
         achieved = flops_per_launch / (k1_avg_ms * 1e-3) / 1e12
-        traffic = ncu_traffic_per_launch(n)
+        exps_per_s = work["exps"] / (k1_avg_ms * 1e-3)
+        traffic = ncu_traffic_per_launch(n, _lib.fp32_operator_kernel(EMBED_DIM))
         line = {
             "metric": METRIC,
             "value": value,
@@ -402,24 +406,8 @@ def run_ours(args) -> None:
                 "h2d_bytes_per_step": int(y_host.numel() * y_host.element_size()),
                 "d2h_bytes_per_step": int(a_host.numel() * a_host.element_size()),
             },
-            "roofline": {
-                "bound": "fma",
-                "kernel": "k1s_matvec_f32 (symmetric FP32 fused matvec)",
-                "achieved": achieved,
-                "peak": peaks["ffma_tflops"],
-                "unit": "TFLOP/s",
-                "frac": achieved / peaks["ffma_tflops"],
-                "traffic": traffic,
-                "avg_launch_ms": k1_avg_ms,
-                "algorithmic_flops_per_launch": flops_per_launch,
-                "entries_evaluated_per_launch": work["entries"],
-                "logical_entries_per_s": n * n / (k1_avg_ms * 1e-3),
-                "peak_source": "FFMA microbenchmark measured in this run (laker_measure_peaks); "
-                               "nominal 148 SM x 128 FMA/clk x 2 flop x clock for context",
-                "nominal_peak_at_max_clock": 148 * 128 * 2 * 1.965e9 / 1e12,
-                "mufu_frac": (work["exps"] / (k1_avg_ms * 1e-3)) / (peaks["mufu_tops"] * 1e12),
-                "fp64_matvec_ms_total": k4_ms,
-            },
+            "roofline": roofline_block(kernel_id, work, k1_avg_ms, achieved, exps_per_s, peaks,
+                                       traffic, n, k4_ms),
             "clocks": clocks.summary(),
             "gpu_launches": launches_all,
         }
@@ -431,6 +419,49 @@ def run_ours(args) -> None:
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def roofline_block(kernel_id, work, k1_avg_ms, achieved, exps_per_s, peaks, traffic, n, k4_ms):
+    """Roofline of the FP32 operator kernel that dominates the solve.
+
+    Tensor-core logits (kernel 2): per entry evaluated the CUDA cores do one
+    MUFU exp2 and two FMAs (one for an entry on a diagonal block pair), so the
+    binding unit is the exp2 rate; the logits add 3 split-TF32 products x 2 x
+    16 flops per entry on the tensor cores.  CUDA-core logits (kernel 1):
+    d + 2 FMAs per entry, bound by the FFMA rate."""
+    common = {
+        "traffic": traffic,
+        "avg_launch_ms": k1_avg_ms,
+        "entries_evaluated_per_launch": work["entries"],
+        "logical_entries_per_s": n * n / (k1_avg_ms * 1e-3),
+        "fp64_matvec_ms_total": k4_ms,
+    }
+    if kernel_id == 2:
+        peak = peaks["mufu_tops"] * 1e12
+        tf32 = work["entries"] * 96.0 / (k1_avg_ms * 1e-3) / 1e12
+        pk = _peaks_file()
+        tf32_peak = pk.get("bf16_tflops", 1590.0) / 2.0
+        return dict(common, **{
+            "bound": "mufu",
+            "kernel": "k1t_matvec (symmetric FP32 operator, split-TF32 tcgen05 logits)",
+            "achieved": exps_per_s / 1e12, "peak": peaks["mufu_tops"], "unit": "Texp2/s",
+            "frac": exps_per_s / peak,
+            "peak_source": "MUFU ex2 microbenchmark measured in this run (laker_measure_peaks)",
+            "fma_flops_per_launch": work["flops"], "fma_frac": achieved / peaks["ffma_tflops"],
+            "tensor_tf32_tflops": tf32, "tensor_frac": tf32 / tf32_peak,
+            "tensor_peak_source": "half the measured cuBLAS bf16 burst (MEASURED_PEAKS.json): TF32 dense",
+        })
+    return dict(common, **{
+        "bound": "fma",
+        "kernel": "k1s_matvec_f32 (symmetric FP32 fused matvec)" if kernel_id == 1
+                  else "k1_matvec_f32 (plain FP32 fused matvec)",
+        "achieved": achieved, "peak": peaks["ffma_tflops"], "unit": "TFLOP/s",
+        "frac": achieved / peaks["ffma_tflops"],
+        "algorithmic_flops_per_launch": work["flops"],
+        "peak_source": "FFMA microbenchmark measured in this run (laker_measure_peaks); "
+                       "nominal 148 SM x 128 FMA/clk x 2 flop x clock for context",
+        "mufu_frac": exps_per_s / (peaks["mufu_tops"] * 1e12),
+    })
 
 
 def kernel_only(args) -> None:

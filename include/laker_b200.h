@@ -109,6 +109,14 @@ int laker_attn_matvec_f32(const float* rows32, int64_t m, const float* cols32, i
  * No counterpart in the reference (roofline accounting). */
 int laker_fp32_matvec_work(int64_t n, int d, double* entries, double* flops, double* exps);
 
+/* Which kernel a square FP32 operator application of dimension d runs:
+ * 0 the plain fused kernel, 1 the symmetric kernel with logits on the CUDA
+ * cores, 2 the symmetric kernel with logits on the tensor cores (split-TF32
+ * tcgen05 MMAs; then `flops` above counts only the CUDA-core accumulation
+ * FMAs and the logits add 3 x 2 x 16 TF32 tensor flops per entry evaluated);
+ * -1 for an invalid d.  No counterpart in the reference. */
+int laker_fp32_operator_kernel(int d);
+
 /* Allocation-free FP32 fused matvec (single right-hand side).
  *   y = lam * x[:m] + exp(Er Ec^T) x          (x: n, y: m)
  * Same arguments and result as laker_attn_matvec_f32 with k = 1, but without

@@ -187,6 +187,7 @@ _SIGNATURES = {
         [c_int64, c_int, POINTER(c_double), POINTER(c_double), POINTER(c_double)],
     ),
     "laker_peaks_scratch_bytes": (c_size_t, []),
+    "laker_fp32_operator_kernel": (c_int, [c_int]),
     "laker_measure_peaks": (
         c_int,
         [_P, POINTER(c_double), POINTER(c_double), POINTER(c_double), _P],
@@ -417,6 +418,11 @@ def fp32_matvec_work(n: int, d: int) -> dict:
     check(load().laker_fp32_matvec_work(n, d, ctypes.byref(e), ctypes.byref(f), ctypes.byref(x)),
           "laker_fp32_matvec_work")
     return {"entries": e.value, "flops": f.value, "exps": x.value}
+
+
+def fp32_operator_kernel(d: int) -> int:
+    """0 plain, 1 symmetric (CUDA-core logits), 2 symmetric (tensor-core logits)."""
+    return int(load().laker_fp32_operator_kernel(d))
 
 
 def measure_peaks(device: torch.device) -> dict:

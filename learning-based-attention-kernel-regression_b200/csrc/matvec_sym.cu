@@ -767,7 +767,8 @@ extern "C" int laker_fp32_matvec_work(int64_t n, int d, double* entries, double*
     const double diag = (double)(sp.nb - 1) * B * B + last * last;
     const double off = (nn - diag) * 0.5;
     e = diag + off;
-    f = 2.0 * (diag * (d + 1) + off * (d + 2));
+    // tensor-core logits: the CUDA cores do only the accumulation FMAs
+    f = k1t_enabled(d) ? 2.0 * (diag + 2.0 * off) : 2.0 * (diag * (d + 1) + off * (d + 2));
   } else {
     e = nn;
     f = 2.0 * nn * (d + 1);
@@ -776,4 +777,10 @@ extern "C" int laker_fp32_matvec_work(int64_t n, int d, double* entries, double*
   if (flops) *flops = f;
   if (exps) *exps = e;
   return LAKER_OK;
+}
+
+extern "C" int laker_fp32_operator_kernel(int d) {
+  if (d < 1 || d > 16) return -1;
+  if (!k1_use_symmetric()) return 0;
+  return k1t_enabled(d) ? 2 : 1;
 }

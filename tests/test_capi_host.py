@@ -48,6 +48,16 @@ def test_argument_validation_without_gpu():
                                      None) == _lib.LAKER_OK
 
 
+def test_operator_kernel_query():
+    from laker_b200 import _lib
+
+    lib = _lib.load()
+    assert lib.laker_fp32_operator_kernel(10) in (0, 1, 2)
+    assert lib.laker_fp32_operator_kernel(16) == lib.laker_fp32_operator_kernel(10)
+    assert lib.laker_fp32_operator_kernel(0) == -1
+    assert lib.laker_fp32_operator_kernel(17) == -1
+
+
 def test_workspace_and_layout_queries():
     from laker_b200 import _lib
 
