@@ -30,6 +30,7 @@
 #include <cstdlib>
 
 #include "internal.cuh"
+#include "sym.cuh"
 #include "tc.cuh"
 
 namespace laker {
@@ -375,6 +376,324 @@ __global__ void __launch_bounds__(kTcThreadsWs, 1)
   }
 }
 
+// ---- logits on the tensor cores (k2t) ------------------------------------------
+// The same items, X image, segment partials and epilogue as k2_tc_matvec, but
+// the kernel entries' logits come from the tensor core too: per column tile
+// the MMA warp issues the six split-TF32 logit MMAs (rows' E, scaled by log2 e,
+// against the tile's points' E, K = 16; operands from the k1t operand image)
+// into one of kSBufs TMEM logit buffers, then the P X products of the previous
+// tile into the O accumulator.  The entry warps read a logit tile from TMEM,
+// apply exp2 (MUFU), split into TF32 hi / lo and write the A operand of P X to
+// shared memory -- no FMAs and no embedding loads per entry on the CUDA cores.
+// TMEM: O in columns [0, 256), logit buffers from column 256.
+constexpr int kSBufs = 4;
+// 16 entry warps in two groups that take alternate tiles (two tiles in flight
+// per row quadrant); group 0 also runs the epilogue.  Then the copy and MMA warps.
+constexpr int kK2tEntry = 512, kK2tThreads = kK2tEntry + 64, kK2tCopyWarp = 16, kK2tMmaWarp = 17;
+constexpr uint32_t kImgVar = 512 * 64;  // one variant of one 512-point image block
+constexpr uint32_t kImgBlock = 4 * kImgVar;
+
+template <bool CLAMP, int TK>
+__global__ void __launch_bounds__(kK2tThreads, 1)
+    k2t_matvec(const uint8_t* __restrict__ rimg, int64_t m, const uint8_t* __restrict__ cimg,
+               const uint8_t* __restrict__ img, int N, int S, int AS, K2Work wk, float lam,
+               const float* __restrict__ X, int64_t ldx, int k, float* __restrict__ Y, int64_t ldy,
+               float* __restrict__ part, int* status) {
+  constexpr int kABytes = TileCfg<TK>::kABytes;
+  constexpr uint32_t kArBytes = kTcRows * 64;   // one variant of the rows' operand
+  constexpr uint32_t kBcBytes = TK * 64;        // one variant of a tile's points' operand
+  static_assert(TK == 32, "logit tiles of 32 points (TMEM buffers of 32 columns)");
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const uint32_t bbytes = (uint32_t)N * (4u * TK);
+  const uint32_t sbytes = (uint32_t)round_up(2 * bbytes + 2 * kBcBytes, 1024);
+  uint8_t* sA = base;                                 // AS P slots x (hi, lo)
+  uint8_t* sAr = sA + (size_t)AS * 2 * kABytes;       // rows' operand (hi, lo)
+  uint8_t* sB = sAr + 2 * kArBytes;                   // S stages: X (hi, lo), points (hi, lo)
+  uint64_t* b_full = reinterpret_cast<uint64_t*>(sB + (size_t)S * sbytes);
+  uint64_t* b_empty = b_full + S;
+  uint64_t* a_full = b_empty + S;
+  uint64_t* a_empty = a_full + AS;
+  uint64_t* s_full = a_empty + AS;
+  uint64_t* s_empty = s_full + kSBufs;
+  uint64_t* acc_full = s_empty + kSBufs;
+  uint64_t* acc_empty = acc_full + 1;
+  uint64_t* ar_full = acc_empty + 1;
+  uint64_t* ar_empty = ar_full + 1;
+  uint64_t* drain = ar_empty + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :
+                 : "r"(smem_u32(tmem_slot)), "r"(512u));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    for (int i = 0; i < S; ++i) {
+      mbar_init(&b_full[i], 1);
+      mbar_init(&b_empty[i], 1);
+    }
+    for (int i = 0; i < AS; ++i) {
+      mbar_init(&a_full[i], kEntryThreads / 32);
+      mbar_init(&a_empty[i], 1);
+    }
+    for (int i = 0; i < kSBufs; ++i) {
+      mbar_init(&s_full[i], 1);
+      mbar_init(&s_empty[i], kEntryThreads / 32);
+    }
+    mbar_init(acc_full, 1);
+    mbar_init(acc_empty, kEntryThreads / 32);  // group 0 runs the epilogue
+    mbar_init(ar_full, 1);
+    mbar_init(ar_empty, 1);
+    mbar_init(drain, 1);
+    *abort = 0;
+    mbar_fence_init();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  auto item_of = [&](int64_t it, int64_t* rt, int* ch, int64_t* t0, int64_t* t1) {
+    *rt = it % wk.rtiles;
+    const int64_t rest = it / wk.rtiles;
+    *ch = (int)(rest % wk.chunks);
+    const int64_t sg = rest / wk.chunks;
+    *t0 = sg * wk.tps;
+    *t1 = *t0 + wk.tps < wk.ntiles ? *t0 + wk.tps : wk.ntiles;
+  };
+  // byte offset of variant v (0, 1: rows scaled hi / lo; 2, 3: points hi / lo)
+  // of point p in the operand image
+  auto img_off = [](int64_t p, int v) -> int64_t {
+    return (p >> 9) * (int64_t)kImgBlock + (int64_t)v * kImgVar + (p & 511) * 64;
+  };
+
+  int64_t b_issued = 0, ar_issued = 0;  // copy role
+  bool mma_any = false;                 // MMA role
+  if (warp == kK2tCopyWarp) {
+    // ---- copies ------------------------------------------------------------
+    if (lane == 0) {
+      int64_t g = 0, ni = 0;
+      for (int64_t it = blockIdx.x; it < wk.items && !*abort; it += gridDim.x, ++ni) {
+        int64_t rt, t0, t1;
+        int ch;
+        item_of(it, &rt, &ch, &t0, &t1);
+        // the rows' operand of this item (released by the MMA after its logits)
+        if (!wait_or_abort(ar_empty, (uint32_t)((ni & 1) ^ 1), status, abort)) break;
+        mbar_arrive_expect_tx(ar_full, 2 * kArBytes);
+        bulk_g2s(sAr, rimg + img_off(rt * kTcRows, 0), kArBytes, ar_full);
+        bulk_g2s(sAr + kArBytes, rimg + img_off(rt * kTcRows, 1), kArBytes, ar_full);
+        ++ar_issued;
+        bool ok = true;
+        for (int64_t t = t0; t < t1; ++t, ++g) {
+          const int st = (int)(g % S);
+          if (!wait_or_abort(&b_empty[st], (uint32_t)(((g / S) & 1) ^ 1), status, abort)) {
+            ok = false;
+            break;
+          }
+          uint8_t* stg = sB + (size_t)st * sbytes;
+          mbar_arrive_expect_tx(&b_full[st], 2 * bbytes + 2 * kBcBytes);
+          bulk_g2s(stg, img + ((int64_t)ch * wk.ntiles + t) * (int64_t)N * (8 * TK), 2 * bbytes, &b_full[st]);
+          bulk_g2s(stg + 2 * bbytes, cimg + img_off(t * TK, 2), kBcBytes, &b_full[st]);
+          bulk_g2s(stg + 2 * bbytes + kBcBytes, cimg + img_off(t * TK, 3), kBcBytes, &b_full[st]);
+          b_issued = g + 1;
+        }
+        if (!ok) break;
+      }
+    }
+  } else if (warp == kK2tMmaWarp) {
+    // ---- MMA issue -----------------------------------------------------------
+    if (lane == 0) {
+      const uint32_t idesc_s = tf32_idesc(TK);  // logits: N = TK points
+      const uint32_t idesc_o = tf32_idesc(N);   // P X: N right-hand sides
+      // descriptors built once and advanced by adds (the start-address field
+      // holds address >> 4; shared addresses stay below 256 KB, so no carry)
+      const uint64_t ar_hi = kmajor_desc_raw(smem_u32(sAr), 512u, 4u);
+      const uint64_t ar_lo = ar_hi + (kArBytes >> 4);
+      const uint64_t p_desc0 = kmajor_desc<TK>(smem_u32(sA));
+      const uint64_t x_desc0 = kmajor_desc<TK>(smem_u32(sB));
+      const uint64_t bc_desc0 = kmajor_desc_raw(smem_u32(sB + 2 * bbytes), 512u, 4u);
+      const uint64_t p_slot_step = (2 * kABytes) >> 4, p_lo_step = kABytes >> 4;
+      const uint64_t stage_step = sbytes >> 4, x_lo_step = bbytes >> 4;
+      int64_t g = 0, ni = 0;
+      bool ok = true;
+      // P X of tile gp (stage / P slot of counter gp); first: the item's first tile
+      auto issue_px = [&](int64_t gp, bool first) -> bool {
+        const int st = (int)(gp % S), as = (int)(gp % AS);
+        if (!wait_or_abort(&a_full[as], (uint32_t)((gp / AS) & 1), status, abort)) return false;
+        tc_fence_after();
+        const uint64_t ahi = p_desc0 + (uint64_t)as * p_slot_step, alo = ahi + p_lo_step;
+        const uint64_t bhi = x_desc0 + (uint64_t)st * stage_step, blo = bhi + x_lo_step;
+#pragma unroll
+        for (int kk = 0; kk < TK / 8; ++kk) {
+          const uint64_t ko = (uint64_t)kk * 2u;  // 32 bytes per 8-point K step
+          mma_tf32(tmem_base, ahi + ko, bhi + ko, idesc_o, (!first || kk > 0) ? 1u : 0u);
+          mma_tf32(tmem_base, ahi + ko, blo + ko, idesc_o, 1u);
+          mma_tf32(tmem_base, alo + ko, bhi + ko, idesc_o, 1u);
+        }
+        mma_commit(&a_empty[as]);
+        mma_commit(&b_empty[st]);
+        return true;
+      };
+      for (int64_t it = blockIdx.x; it < wk.items && ok && !*abort; it += gridDim.x, ++ni) {
+        int64_t rt, t0, t1;
+        int ch;
+        item_of(it, &rt, &ch, &t0, &t1);
+        (void)rt;
+        (void)ch;
+        if (!wait_or_abort(ar_full, (uint32_t)(ni & 1), status, abort) ||
+            !wait_or_abort(acc_empty, (uint32_t)((ni & 1) ^ 1), status, abort)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        // logits run up to L tiles ahead of the P X products (L <= S: a tile's
+        // stage is held from its logits to its P X; L <= kSBufs: TMEM buffers)
+        const int L = S < kSBufs ? S : kSBufs;
+        const int64_t g0 = g, n_t = t1 - t0;
+        int64_t gl = g0;  // next tile (counter) whose logits are issued
+        for (int64_t gp = g0; gp < g0 + n_t; ++gp) {
+          for (; gl < g0 + n_t && gl < gp + L; ++gl) {
+            const int st = (int)(gl % S), sb = (int)(gl % kSBufs);
+            if (!wait_or_abort(&b_full[st], (uint32_t)((gl / S) & 1), status, abort) ||
+                !wait_or_abort(&s_empty[sb], (uint32_t)(((gl / kSBufs) & 1) ^ 1), status, abort)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint64_t bc_hi = bc_desc0 + (uint64_t)st * stage_step, bc_lo = bc_hi + (kBcBytes >> 4);
+            const uint32_t ds = tmem_base + 256u + (uint32_t)(sb * TK);
+#pragma unroll
+            for (int kk = 0; kk < 2; ++kk) {
+              const uint64_t ko = (uint64_t)kk * 2u;  // 32 bytes in the start-address field
+              mma_tf32(ds, ar_hi + ko, bc_hi + ko, idesc_s, kk > 0 ? 1u : 0u);
+              mma_tf32(ds, ar_hi + ko, bc_lo + ko, idesc_s, 1u);
+              mma_tf32(ds, ar_lo + ko, bc_hi + ko, idesc_s, 1u);
+            }
+            mma_any = true;
+            mma_commit(&s_full[sb]);
+            if (gl + 1 == g0 + n_t) mma_commit(ar_empty);  // last logits of the item issued
+          }
+          if (!ok || !issue_px(gp, gp == g0)) {
+            ok = false;
+            break;
+          }
+        }
+        g = g0 + n_t;
+        if (!ok) break;
+        mma_commit(acc_full);
+      }
+    }
+  } else {
+    // ---- entries (warps 0-15: group warp >> 3 takes tiles g with g & 1 ==
+    // group) + epilogue (group 0) -------------------------------------------
+    const int grp = warp >> 3;
+    const int q = warp & 3, h = (warp >> 2) & 1;
+    const int row = q * 32 + lane;  // TMEM lane = row of the tile
+    const uint32_t lane_base = (uint32_t)(q * 32) << 16;
+    int64_t g = 0, ni = 0;
+    for (int64_t it = blockIdx.x; it < wk.items; it += gridDim.x, ++ni) {
+      if (__any_sync(0xffffffffu, *abort != 0)) break;
+      int64_t rt, t0, t1;
+      int ch;
+      item_of(it, &rt, &ch, &t0, &t1);
+      bool ok = true;
+      for (int64_t t = t0; t < t1; ++t, ++g) {
+        if ((int)(g & 1) != grp) continue;
+        const int as = (int)(g % AS), sb = (int)(g % kSBufs);
+        if (!__all_sync(0xffffffffu, wait_or_abort(&s_full[sb], (uint32_t)((g / kSBufs) & 1), status, abort))) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        float v[16];
+        tmem_ld16(tmem_base + lane_base + 256u + (uint32_t)(sb * TK + h * 16), v);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&s_empty[sb]);
+        if (!__all_sync(0xffffffffu,
+                        wait_or_abort(&a_empty[as], (uint32_t)(((g / AS) & 1) ^ 1), status, abort))) {
+          ok = false;
+          break;
+        }
+        uint8_t* a_hi = sA + (size_t)as * 2 * kABytes;
+        uint8_t* a_lo = a_hi + kABytes;
+#pragma unroll
+        for (int c4 = 0; c4 < 4; ++c4) {
+          uint4 hi, lo;
+          uint32_t* ph = &hi.x;
+          uint32_t* pl = &lo.x;
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const float sv = v[4 * c4 + u];
+            const float p = ex2_approx(CLAMP ? fminf(sv, kClampLog2) : sv);
+            ph[u] = to_tf32(p);
+            pl[u] = to_tf32(p - __uint_as_float(ph[u]));
+          }
+          const uint32_t off = TileCfg<TK>::offset((uint32_t)row, (uint32_t)(h * 16 + 4 * c4));
+          *reinterpret_cast<uint4*>(a_hi + off) = hi;
+          *reinterpret_cast<uint4*>(a_lo + off) = lo;
+        }
+        fence_async_smem();  // this thread's entries -> visible to the tensor core
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&a_full[as]);
+      }
+      if (!ok) break;
+      if (grp != 0) continue;
+      // epilogue: this item's accumulators
+      if (!__all_sync(0xffffffffu, wait_or_abort(acc_full, (uint32_t)(ni & 1), status, abort))) break;
+      tc_fence_after();
+      const int64_t r = rt * kTcRows + row;
+      const int nh = N / 2, c_begin = h * nh;
+      const int sg = (int)(t0 / wk.tps);
+      for (int c0 = c_begin; c0 < c_begin + nh; c0 += 16) {
+        float o[16];
+        tmem_ld16(tmem_base + lane_base + (uint32_t)c0, o);
+        if (r < m) {
+#pragma unroll
+          for (int u = 0; u < 16; ++u) {
+            const int qq = ch * N + c0 + u;
+            if (qq < k) {
+              if (wk.segs == 1)
+                Y[r * ldy + qq] = o[u] + (lam != 0.0f ? lam * X[r * ldx + qq] : 0.0f);
+              else
+                part[((int64_t)sg * m + r) * k + qq] = o[u];
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(acc_empty);
+    }
+  }
+
+  // ---- teardown: every role has left its loop ---------------------------------
+  __syncthreads();
+  if (*abort) {
+    // bounded drains of the copies in flight and of the MMAs issued
+    if (warp == kK2tCopyWarp && lane == 0) {
+      if (ar_issued > 0) mbar_wait_bounded(ar_full, (uint32_t)((ar_issued - 1) & 1), status);
+      const int64_t from = b_issued > S ? b_issued - S : 0;
+      for (int64_t gg = from; gg < b_issued; ++gg)
+        mbar_wait_bounded(&b_full[gg % S], (uint32_t)((gg / S) & 1), status);
+    }
+    if (warp == kK2tMmaWarp && lane == 0 && mma_any) {
+      mma_commit(drain);
+      mbar_wait_bounded(drain, 0u, status);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" : : "r"(tmem_base), "r"(512u));
+  }
+}
+
 // Y = lam X + sum over segments of the partials, in segment order.
 __global__ void k2_reduce_kernel(const float* __restrict__ part, int segs, int64_t m, int k,
                                  float lam, const float* __restrict__ X, int64_t ldx,
@@ -468,6 +787,41 @@ cudaError_t launch_k2_tk(const float* rows32, int64_t m, const float* cols32, co
                                     status, s);
 }
 
+// Logit-on-tensor-core variant: P slots (2 for wide chunks, 4 for narrow
+// ones) and as many B stages as fit, 2..8.
+int k2t_pslots(int N) { return N > 128 ? 2 : 4; }
+
+int k2t_stages(int N, int AS) {
+  const int sb = (int)round_up(2 * N * 4 * 32 + 2 * 32 * 64, 1024);
+  const int avail = 227 * 1024 - 1024 - AS * 2 * kTcRows * 32 * 4 - 2 * kTcRows * 64 - 512;
+  int S = avail / sb;
+  if (S > kTcMaxStages) S = kTcMaxStages;
+  return S;
+}
+
+size_t k2t_smem_bytes(int N, int S, int AS) {
+  const size_t sb = (size_t)round_up(2 * N * 4 * 32 + 2 * 32 * 64, 1024);
+  return 1024 + (size_t)AS * 2 * kTcRows * 32 * 4 + 2 * kTcRows * 64 + (size_t)S * sb +
+         (size_t)(2 * S + 2 * AS + 2 * kSBufs + 5) * 8 + 16;
+}
+
+template <bool CLAMP>
+cudaError_t launch_k2t_t(const uint8_t* rimg, int64_t m, const uint8_t* cimg, const uint8_t* img,
+                         int N, const K2Work& wk, float lam, const float* X, int64_t ldx, int k,
+                         float* Y, int64_t ldy, float* part, int* status, cudaStream_t s) {
+  const int AS = k2t_pslots(N);
+  const int S = k2t_stages(N, AS);
+  const size_t smem = k2t_smem_bytes(N, S, AS);
+  if (S < 2 || smem > 227 * 1024) return cudaErrorInvalidConfiguration;
+  auto fn = k2t_matvec<CLAMP, 32>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int64_t grid = wk.items < (int64_t)sm_count() ? wk.items : (int64_t)sm_count();
+  fn<<<(unsigned)grid, kK2tThreads, smem, s>>>(rimg, m, cimg, img, N, S, AS, wk, lam, X, ldx, k, Y,
+                                               ldy, part, status);
+  return cudaGetLastError();
+}
+
 }  // namespace
 
 // RHS per CTA for k right-hand sides: a multiple of 32 (the MMA's N for M =
@@ -478,14 +832,38 @@ int k2_chunk_cols(int k) {
   return (int)round_up(kk, 32);
 }
 
-// Workspace of one multi-RHS product: the split X image, then the segment
-// partials when the column range is split.
+// Whether the multi-RHS kernel takes its logits from the tensor cores too
+// (k2t, LAKER_K2_LOGITS_TC=1).  Off by default: measured on B200 it matches
+// k2_tc_matvec for narrow chunks (n = 50k, k = 16: 7.07 vs 7.31 ms) and is
+// slower for wide ones (n = 20k, k = 256: 2.17 vs 1.49 ms); both are bound by
+// their pipelines (mbarrier polling dominates the issued instructions), not
+// by the entry arithmetic that k2t moves to the tensor cores.
+bool k2_logits_tc() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("LAKER_K2_LOGITS_TC");
+    v = (e && e[0] == '1') ? 1 : 0;
+  }
+  return v == 1;
+}
+
+namespace {
+int k2_tk_for(int N) { return k2_logits_tc() ? 32 : k2_tile_points(N); }
+size_t k2_x_image_bytes(const K2Work& w, int N, int TK) {
+  return (size_t)round_up((int64_t)((size_t)(w.chunks * w.ntiles) * (size_t)N * 8 * TK), 256);
+}
+}  // namespace
+
+// Workspace of one multi-RHS product: the split X image, the segment
+// partials when the column range is split, and (tensor-core logits) the
+// operand images of the rows' and the points' embeddings.
 size_t k2_image_bytes(int64_t m, int64_t n, int k) {
   const int N = k2_chunk_cols(k);
-  const int TK = k2_tile_points(N);
+  const int TK = k2_tk_for(N);
   const K2Work w = k2_work(m, n, k, N, TK);
-  size_t b = (size_t)round_up((int64_t)((size_t)(w.chunks * w.ntiles) * (size_t)N * 8 * TK), 256);
-  if (w.segs > 1) b += (size_t)w.segs * (size_t)m * (size_t)k * 4;
+  size_t b = k2_x_image_bytes(w, N, TK);
+  if (w.segs > 1) b += (size_t)round_up((int64_t)((size_t)w.segs * (size_t)m * (size_t)k * 4), 1024);
+  if (k2_logits_tc()) b += k1t_image_bytes(m) + k1t_image_bytes(n);
   return b;
 }
 
@@ -504,12 +882,12 @@ cudaError_t launch_k2(const float* rows32, int64_t m, const float* cols32, int64
                       int clamp, float lam, const float* X, int64_t ldx, int k, float* Y,
                       int64_t ldy, uint8_t* img, int* status, cudaStream_t s) {
   const int N = k2_chunk_cols(k);
-  const int TK = k2_tile_points(N);
+  const int TK = k2_tk_for(N);
   const K2Work wk = k2_work(m, n, k, N, TK);
-  float* part = wk.segs > 1
-                    ? reinterpret_cast<float*>(img + round_up((int64_t)((size_t)(wk.chunks * wk.ntiles) *
-                                                                        (size_t)N * 8 * TK), 256))
-                    : nullptr;
+  const size_t xbytes = k2_x_image_bytes(wk, N, TK);
+  float* part = wk.segs > 1 ? reinterpret_cast<float*>(img + xbytes) : nullptr;
+  const size_t pbytes =
+      wk.segs > 1 ? (size_t)round_up((int64_t)((size_t)wk.segs * (size_t)m * (size_t)k * 4), 1024) : 0;
   {
     const int64_t total = wk.ntiles * TK * (int64_t)wk.chunks * N;
     int64_t g = ceil_div(total, 256);
@@ -523,7 +901,21 @@ cudaError_t launch_k2(const float* rows32, int64_t m, const float* cols32, int64
   }
   const int dp = padded_dim(d);
   cudaError_t e = cudaErrorInvalidValue;
-  if (clamp) {
+  if (k2_logits_tc()) {
+    // operand images of the rows and of the points (one image for a square
+    // product with the same embeddings)
+    uint8_t* rimg = img + xbytes + pbytes;
+    uint8_t* cimg = rimg;
+    const int64_t rrows = round_up(m > 0 ? m : 1, 512), crows = round_up(n > 0 ? n : 1, 512);
+    e = launch_k1t_pack(rows32, m, d, rimg, rrows, s);
+    if (e == cudaSuccess && !(rows32 == cols32 && m == n)) {
+      cimg = rimg + k1t_image_bytes(m);
+      e = launch_k1t_pack(cols32, n, d, cimg, crows, s);
+    }
+    if (e == cudaSuccess)
+      e = clamp ? launch_k2t_t<true>(rimg, m, cimg, img, N, wk, lam, X, ldx, k, Y, ldy, part, status, s)
+                : launch_k2t_t<false>(rimg, m, cimg, img, N, wk, lam, X, ldx, k, Y, ldy, part, status, s);
+  } else if (clamp) {
     LAKER_DISPATCH_TC(dp, e = (launch_k2_tk<DPv, true>(rows32, m, cols32, img, N, TK, wk, lam, X, ldx, k, Y, ldy, part, status, s)));
   } else {
     LAKER_DISPATCH_TC(dp, e = (launch_k2_tk<DPv, false>(rows32, m, cols32, img, N, TK, wk, lam, X, ldx, k, Y, ldy, part, status, s)));
