@@ -448,10 +448,8 @@ __global__ void __launch_bounds__(kTThreads, 1)
 #pragma unroll
         for (int hp = 0; hp < kTRowTiles / UT; ++hp, ++g) {
           const int buf = (int)(g % kTBufs);
-          if (!dead) {
-            const bool ok = wait_or_abort(&acc_full[buf], (uint32_t)((g / kTBufs) & 1), status, abort);
-            dead = !__all_sync(0xffffffffu, ok);
-          }
+          if (!dead)
+            dead = !warp_wait_or_abort(&acc_full[buf], (uint32_t)((g / kTBufs) & 1), status, abort, lane);
           if (!dead) {
             tc_fence_after();
             const uint32_t t0 = tmem_base + lane_base + (uint32_t)(buf * (UT * kTSlabN) + cg * CW);

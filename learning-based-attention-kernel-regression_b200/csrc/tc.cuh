@@ -143,4 +143,19 @@ __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, in
   return false;
 }
 
+// Warp-wide wait: lane 0 polls (one poll per warp instead of 32), then every
+// lane confirms the completed phase with its own try_wait, which also gives
+// each lane the acquire ordering.  The phase cannot advance again before this
+// warp releases the resource it guards, so the confirmation succeeds at once;
+// should it not, the lane falls back to the bounded wait.  All 32 lanes must
+// call it; the result is warp-uniform.
+__device__ __forceinline__ bool warp_wait_or_abort(uint64_t* bar, uint32_t parity, int* status,
+                                                   volatile int* abort, int lane) {
+  bool ok = true;
+  if (lane == 0) ok = wait_or_abort(bar, parity, status, abort);
+  ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+  if (ok && !mbar_try_wait(bar, parity)) ok = wait_or_abort(bar, parity, status, abort);
+  return __all_sync(0xffffffffu, ok);
+}
+
 }  // namespace laker
