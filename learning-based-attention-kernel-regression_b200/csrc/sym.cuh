@@ -70,16 +70,29 @@ __host__ __device__ inline void sym_pair_coords(int64_t p, int64_t nb, int64_t* 
 // pairs (a' < a, a), in that fixed order.  Both partial arrays hold one
 // B-vector per pair (FP32 kernel: double row sums, float column sums; FP64
 // kernel: both double).
+// The terms go round-robin into four partial sums (independent chains, so
+// the loads overlap), combined as (s0 + s1) + (s2 + s3): a fixed order.
 template <typename RP, typename CP>
 __device__ inline double sym_instance_row_sum(int64_t nb, int64_t ps, int B,
                                               const RP* __restrict__ rowpart,
                                               const CP* __restrict__ colpart, int64_t li) {
   const int64_t a = li / B, o = li - a * B;
   const int64_t f = ps + sym_first_pair(a, nb);
-  double s = 0.0;
-  for (int64_t q = 0; q < nb - a; ++q) s += (double)rowpart[(f + q) * B + o];
-  for (int64_t ap = 0; ap < a; ++ap) s += (double)colpart[(ps + sym_pair_index(ap, a, nb)) * B + o];
-  return s;
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+  const int64_t nq = nb - a;
+  int64_t q = 0;
+  for (; q + 4 <= nq; q += 4) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) s[u] += (double)rowpart[(f + q + u) * B + o];
+  }
+  for (int u = 0; q < nq; ++q, ++u) s[u] += (double)rowpart[(f + q) * B + o];
+  int64_t ap = 0;
+  for (; ap + 4 <= a; ap += 4) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) s[u] += (double)colpart[(ps + sym_pair_index(ap + u, a, nb)) * B + o];
+  }
+  for (int u = 0; ap < a; ++ap, ++u) s[u] += (double)colpart[(ps + sym_pair_index(ap, a, nb)) * B + o];
+  return (s[0] + s[1]) + (s[2] + s[3]);
 }
 
 // Single instance.
