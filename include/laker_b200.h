@@ -117,6 +117,26 @@ int laker_fp32_matvec_work(int64_t n, int d, double* entries, double* flops, dou
  * -1 for an invalid d.  No counterpart in the reference. */
 int laker_fp32_operator_kernel(int d);
 
+/* Kernel variant choices, changeable between calls (no call may be in flight
+ * on any stream): they start from the environment switches and are what the
+ * autotuner sets after timing the candidates on the caller's problem size.
+ *   LAKER_VARIANT_K1T_UNIT       TMEM unit of the tensor-core symmetric
+ *                                operator: 4 (default) or 2 row tiles
+ *   LAKER_VARIANT_K2_LOGITS_N32  multi-RHS chunks of <= 32 right-hand sides,
+ *   LAKER_VARIANT_K2_LOGITS_N128 of 33..128, and
+ *   LAKER_VARIANT_K2_LOGITS_WIDE of more than 128: 0 logits on the CUDA cores
+ *                                (default), 1 logits on the tensor cores
+ * laker_set_variant returns the previous value, or -1 (nothing changed) for
+ * an unknown `which` or an invalid value; laker_get_variant returns the
+ * current value (-1 for an unknown `which`).  No counterpart in the
+ * reference. */
+#define LAKER_VARIANT_K1T_UNIT 0
+#define LAKER_VARIANT_K2_LOGITS_N32 1
+#define LAKER_VARIANT_K2_LOGITS_N128 2
+#define LAKER_VARIANT_K2_LOGITS_WIDE 3
+int laker_set_variant(int which, int value);
+int laker_get_variant(int which);
+
 /* Allocation-free FP32 fused matvec (single right-hand side).
  *   y = lam * x[:m] + exp(Er Ec^T) x          (x: n, y: m)
  * Same arguments and result as laker_attn_matvec_f32 with k = 1, but without

@@ -27,6 +27,7 @@ from .models import LAKERRegressor
 from .preconditioner import CCCPPreconditioner, adaptive_shrinkage_rho, eigh_stable
 from .solvers import PreconditionedConjugateGradient
 from .batched import BatchedPCG, build_cccp_batched
+from .autotune import autotune
 from .engine import EngineCapacityError, SolveEngine, engine_bytes_per_instance
 
 __version__ = "0.1.0"
@@ -40,6 +41,7 @@ def build(force: bool = False, verbose: bool = False):
 
 
 __all__ = [
+    "autotune",
     "AttentionKernelOperator",
     "BatchedPCG",
     "build_cccp_batched",

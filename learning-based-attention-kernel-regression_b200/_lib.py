@@ -188,6 +188,8 @@ _SIGNATURES = {
     ),
     "laker_peaks_scratch_bytes": (c_size_t, []),
     "laker_fp32_operator_kernel": (c_int, [c_int]),
+    "laker_set_variant": (c_int, [c_int, c_int]),
+    "laker_get_variant": (c_int, [c_int]),
     "laker_measure_peaks": (
         c_int,
         [_P, POINTER(c_double), POINTER(c_double), POINTER(c_double), _P],
@@ -418,6 +420,28 @@ def fp32_matvec_work(n: int, d: int) -> dict:
     check(load().laker_fp32_matvec_work(n, d, ctypes.byref(e), ctypes.byref(f), ctypes.byref(x)),
           "laker_fp32_matvec_work")
     return {"entries": e.value, "flops": f.value, "exps": x.value}
+
+
+# kernel variant slots (include/laker_b200.h, LAKER_VARIANT_*)
+VARIANT_K1T_UNIT = 0
+VARIANT_K2_LOGITS_N32 = 1
+VARIANT_K2_LOGITS_N128 = 2
+VARIANT_K2_LOGITS_WIDE = 3
+
+
+def set_variant(which: int, value: int) -> int:
+    """Set a kernel variant choice; returns the previous value."""
+    prev = int(load().laker_set_variant(which, value))
+    if prev < 0:
+        raise ValueError(f"invalid kernel variant {which} = {value}")
+    return prev
+
+
+def get_variant(which: int) -> int:
+    v = int(load().laker_get_variant(which))
+    if v < 0:
+        raise ValueError(f"unknown kernel variant {which}")
+    return v
 
 
 def fp32_operator_kernel(d: int) -> int:

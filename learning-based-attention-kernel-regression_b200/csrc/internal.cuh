@@ -61,4 +61,7 @@ cudaError_t launch_k2(const float* rows32, int64_t m, const float* cols32, int64
                       int clamp, float lam, const float* X, int64_t ldx, int k, float* Y,
                       int64_t ldy, uint8_t* img, int* status, cudaStream_t s);
 
+// Current kernel variant choice (variants.cu; LAKER_VARIANT_* in the header).
+int variant_get(int which);
+
 }  // namespace laker

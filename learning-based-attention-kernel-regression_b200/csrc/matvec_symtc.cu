@@ -541,15 +541,9 @@ cudaError_t launch_k1t_t(const uint8_t* img, int64_t n, const float* x, double* 
   return cudaGetLastError();
 }
 
-// Row tiles per TMEM unit: 4 (default) or 2 (LAKER_K1T_UNIT=2).
-int k1t_unit_tiles() {
-  static int v = 0;
-  if (v == 0) {
-    const char* e = getenv("LAKER_K1T_UNIT");
-    v = (e && e[0] == '2' && e[1] == 0) ? 2 : 4;
-  }
-  return v;
-}
+// Row tiles per TMEM unit: 4 (default) or 2 (LAKER_K1T_UNIT=2 or
+// laker_set_variant).
+int k1t_unit_tiles() { return variant_get(LAKER_VARIANT_K1T_UNIT); }
 
 template <bool CLAMP, bool BATCHED>
 cudaError_t launch_k1t_ut(const uint8_t* img, int64_t n, const float* x, double* rowpart,

@@ -832,23 +832,22 @@ int k2_chunk_cols(int k) {
   return (int)round_up(kk, 32);
 }
 
-// Whether the multi-RHS kernel takes its logits from the tensor cores too
-// (k2t, LAKER_K2_LOGITS_TC=1).  Off by default: measured on B200 it matches
-// k2_tc_matvec for narrow chunks (n = 50k, k = 16: 7.07 vs 7.31 ms) and is
-// slower for wide ones (n = 20k, k = 256: 2.17 vs 1.49 ms); both are bound by
-// their pipelines (mbarrier polling dominates the issued instructions), not
-// by the entry arithmetic that k2t moves to the tensor cores.
-bool k2_logits_tc() {
-  static int v = -1;
-  if (v < 0) {
-    const char* e = getenv("LAKER_K2_LOGITS_TC");
-    v = (e && e[0] == '1') ? 1 : 0;
-  }
-  return v == 1;
+// Whether the multi-RHS kernel for chunks of N right-hand sides takes its
+// logits from the tensor cores too (k2t; LAKER_K2_LOGITS_TC=1 or
+// laker_set_variant per chunk-width class).  Off by default: measured on B200
+// it matches k2_tc_matvec for narrow chunks (n = 50k, k = 16: 7.07 vs 7.31 ms)
+// and is slower for wide ones (n = 20k, k = 256: 2.17 vs 1.49 ms); both are
+// bound by their pipelines (mbarrier polling dominates the issued
+// instructions), not by the entry arithmetic that k2t moves to the tensor
+// cores.  The autotuner picks per class on the caller's sizes.
+bool k2_logits_tc(int N) {
+  const int which = N <= 32 ? LAKER_VARIANT_K2_LOGITS_N32
+                            : (N <= 128 ? LAKER_VARIANT_K2_LOGITS_N128 : LAKER_VARIANT_K2_LOGITS_WIDE);
+  return variant_get(which) == 1;
 }
 
 namespace {
-int k2_tk_for(int N) { return k2_logits_tc() ? 32 : k2_tile_points(N); }
+int k2_tk_for(int N) { return k2_logits_tc(N) ? 32 : k2_tile_points(N); }
 size_t k2_x_image_bytes(const K2Work& w, int N, int TK) {
   return (size_t)round_up((int64_t)((size_t)(w.chunks * w.ntiles) * (size_t)N * 8 * TK), 256);
 }
@@ -863,7 +862,7 @@ size_t k2_image_bytes(int64_t m, int64_t n, int k) {
   const K2Work w = k2_work(m, n, k, N, TK);
   size_t b = k2_x_image_bytes(w, N, TK);
   if (w.segs > 1) b += (size_t)round_up((int64_t)((size_t)w.segs * (size_t)m * (size_t)k * 4), 1024);
-  if (k2_logits_tc()) b += k1t_image_bytes(m) + k1t_image_bytes(n);
+  if (k2_logits_tc(N)) b += k1t_image_bytes(m) + k1t_image_bytes(n);
   return b;
 }
 
@@ -901,7 +900,7 @@ cudaError_t launch_k2(const float* rows32, int64_t m, const float* cols32, int64
   }
   const int dp = padded_dim(d);
   cudaError_t e = cudaErrorInvalidValue;
-  if (k2_logits_tc()) {
+  if (k2_logits_tc(N)) {
     // operand images of the rows and of the points (one image for a square
     // product with the same embeddings)
     uint8_t* rimg = img + xbytes + pbytes;

@@ -1,0 +1,54 @@
+// Run-time kernel variant choices.  Each starts from its environment switch
+// (read once) and can be changed between calls with laker_set_variant, which
+// is what the autotuner (laker_b200.autotune) does after timing the candidates
+// on the caller's problem size.
+#include <atomic>
+#include <cstdlib>
+
+#include "internal.cuh"
+
+namespace laker {
+namespace {
+
+constexpr int kNumVariants = 4;
+std::atomic<int> g_variant[kNumVariants] = {{-1}, {-1}, {-1}, {-1}};
+
+int variant_default(int which) {
+  if (which == LAKER_VARIANT_K1T_UNIT) {
+    const char* e = getenv("LAKER_K1T_UNIT");
+    return (e && e[0] == '2' && e[1] == 0) ? 2 : 4;
+  }
+  const char* e = getenv("LAKER_K2_LOGITS_TC");
+  return (e && e[0] == '1') ? 1 : 0;
+}
+
+bool variant_valid(int which, int value) {
+  if (which == LAKER_VARIANT_K1T_UNIT) return value == 2 || value == 4;
+  return value == 0 || value == 1;
+}
+
+}  // namespace
+
+int variant_get(int which) {
+  if (which < 0 || which >= kNumVariants) return -1;
+  int v = g_variant[which].load(std::memory_order_relaxed);
+  if (v < 0) {
+    v = variant_default(which);
+    int expected = -1;
+    if (!g_variant[which].compare_exchange_strong(expected, v)) v = expected;
+  }
+  return v;
+}
+
+}  // namespace laker
+
+using namespace laker;
+
+extern "C" int laker_set_variant(int which, int value) {
+  if (which < 0 || which >= kNumVariants || !variant_valid(which, value)) return -1;
+  const int prev = variant_get(which);
+  g_variant[which].store(value, std::memory_order_relaxed);
+  return prev;
+}
+
+extern "C" int laker_get_variant(int which) { return variant_get(which); }

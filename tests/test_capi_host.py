@@ -58,6 +58,25 @@ def test_operator_kernel_query():
     assert lib.laker_fp32_operator_kernel(17) == -1
 
 
+def test_variant_switches_without_gpu():
+    from laker_b200 import _lib
+
+    lib = _lib.load()
+    unit = lib.laker_get_variant(_lib.VARIANT_K1T_UNIT)
+    assert unit in (2, 4)
+    assert lib.laker_set_variant(_lib.VARIANT_K1T_UNIT, 3) == -1  # invalid: unchanged
+    assert lib.laker_get_variant(_lib.VARIANT_K1T_UNIT) == unit
+    assert lib.laker_set_variant(_lib.VARIANT_K1T_UNIT, 2) == unit
+    assert lib.laker_set_variant(_lib.VARIANT_K1T_UNIT, unit) == 2
+    for slot in (_lib.VARIANT_K2_LOGITS_N32, _lib.VARIANT_K2_LOGITS_N128, _lib.VARIANT_K2_LOGITS_WIDE):
+        v = lib.laker_get_variant(slot)
+        assert v in (0, 1)
+        assert lib.laker_set_variant(slot, 2) == -1
+        assert lib.laker_set_variant(slot, 1 - v) == v
+        assert lib.laker_set_variant(slot, v) == 1 - v
+    assert lib.laker_get_variant(9) == -1 and lib.laker_set_variant(9, 0) == -1
+
+
 def test_workspace_and_layout_queries():
     from laker_b200 import _lib
 
