@@ -6,7 +6,8 @@ Drop-in for the solve-path surface of laker.models.LAKERRegressor
 core, fit / predict / predict_variance / score / score_r2 / get_params /
 set_params, and the fitted attributes (embeddings, alpha, kernel_operator,
 preconditioner, embedding_model, pcg_iterations_, x_train, y_train).
-Training, search, streaming and persistence helpers are outside the solve path
+save / load round-trip a fitted model (persistence.py; the CCCP factors
+included).  Training, search and streaming helpers are outside the solve path
 and raise NotImplementedError.
 """
 
@@ -26,7 +27,7 @@ logger = logging.getLogger(__name__)
 _OUT_OF_SCOPE = (
     "fit_with_search", "fit_with_bo", "partial_fit", "fit_path", "fit_continuation",
     "fit_learned_embeddings", "fit_residual_corrector", "fit_bilevel", "fit_uncertainty_aware",
-    "condition_number", "save",
+    "condition_number",
 )
 
 
@@ -196,6 +197,9 @@ class LAKERRegressor:
         x = to_tensor(x, device=self.device, dtype=self.dtype)
         if x.dim() != 2:
             raise ValueError(f"x must be 2-D, got shape {x.shape}")
+        if self.preconditioner is None:  # e.g. loaded from a file without CCCP factors
+            self.preconditioner = self.core.build_preconditioner(
+                self.kernel_operator.matvec, self.embeddings.shape[0], diagonal=None)
         return self.core.predict_variance(x, self.embedding_model, self.embeddings,
                                           self.kernel_operator, self.preconditioner, self.alpha,
                                           self.lambda_reg)
@@ -215,6 +219,20 @@ class LAKERRegressor:
         if ss_tot.item() == 0.0:
             return 1.0 if ss_res.item() == 0.0 else 0.0
         return (1.0 - ss_res / ss_tot).item()
+
+    def save(self, path: str) -> None:
+        """Serialise the fitted model (models.py:851-864; persistence.py)."""
+        from .persistence import ModelPersistence
+
+        ModelPersistence.save(self, path)
+
+    @classmethod
+    def load(cls, path: str, device=None) -> "LAKERRegressor":
+        """Rebuild a model written by save (models.py:866-882; persistence.py);
+        `device` overrides the stored one (a file saved on a CPU host)."""
+        from .persistence import ModelPersistence
+
+        return ModelPersistence.load(path, device=device)
 
     def get_params(self, deep: bool = True) -> dict:
         """Constructor parameters (models.py:778-824)."""

@@ -298,6 +298,42 @@ class CCCPPreconditioner:
         self._c = _lib.precond_struct(self._q32, self._w32, self.n, self.nr,
                                       self.isotropic_coef ** (-0.5))
 
+    # ---- persistence ----------------------------------------------------------
+    def state_dict(self) -> dict:
+        """The built state, on the CPU: hyperparameters, the factors of the
+        reference state (q_basis, qr_r, isotropic_coef, q_basis_matrix) and the
+        folded FP32 apply core W exactly as the fused apply uses it."""
+        if self._c is None:
+            raise RuntimeError("Preconditioner has not been built. Call build() first.")
+        cpu = lambda t: t.detach().to("cpu") if torch.is_tensor(t) else t  # noqa: E731
+        return {
+            "num_probes": self.num_probes, "gamma": self.gamma, "epsilon": self.epsilon,
+            "base_rho": self.base_rho, "max_iter": self.max_iter, "tol": self.tol,
+            "n": self.n, "nr": self.nr, "isotropic_coef": float(self.isotropic_coef),
+            "cccp_iterations": int(self.cccp_iterations),
+            "q_basis": cpu(self.q_basis), "qr_r": cpu(self.qr_r),
+            "q_basis_matrix": cpu(self.q_basis_matrix), "w32": cpu(self._w32),
+        }
+
+    @classmethod
+    def from_state(cls, state: dict, device=None, dtype=None) -> "CCCPPreconditioner":
+        """A built preconditioner from state_dict() output (no rebuild: the
+        apply uses the stored factors, so results are the same bits)."""
+        pre = cls(num_probes=state["num_probes"], gamma=state["gamma"], epsilon=state["epsilon"],
+                  base_rho=state["base_rho"], max_iter=state["max_iter"], tol=state["tol"],
+                  verbose=False, device=device, dtype=dtype)
+        dev = pre.device
+        pre.n, pre.nr = int(state["n"]), int(state["nr"])
+        pre.isotropic_coef = float(state["isotropic_coef"])
+        pre.cccp_iterations = int(state["cccp_iterations"])
+        pre.q_basis = state["q_basis"].to(dev)
+        pre.qr_r = state["qr_r"].to(dev) if state.get("qr_r") is not None else None
+        pre.q_basis_matrix = state["q_basis_matrix"].to(dev)
+        pre._q32 = _lib.padded_q(pre.q_basis)
+        pre._w32 = state["w32"].to(dev, torch.float32).contiguous()
+        pre._c = _lib.precond_struct(pre._q32, pre._w32, pre.n, pre.nr, pre.isotropic_coef ** (-0.5))
+        return pre
+
     def c_precond(self) -> _lib.laker_precond:
         if self._c is None:
             raise RuntimeError("Preconditioner has not been built. Call build() first.")
