@@ -66,6 +66,52 @@ class PackedEmbeddings:
         self.packed64 = _lib.pack_f64(E.detach())
 
 
+class _AttnMatvec(torch.autograd.Function):
+    """y = (lambda I + G) x with G = exp(E E^T), differentiable in E and x.
+
+    For a loss with upstream gradient Y' (same shape as y):
+      dL/dx = (lambda I + G) Y'                        (G is symmetric)
+      dL/de_i = sum_c [ Y'_ic (G (x_c * E))_i + x_ic (G (Y'_c * E))_i ]
+    (d/de_i of exp(e_i . e_j) = exp(e_i . e_j) e_j, and e_i appears in row i
+    and column i).  The E gradient is one multi-RHS product of G with the 2 k d
+    columns x_c * E and Y'_c * E -- the fused multi-RHS kernel, in chunks.
+    Entries clamped before exp (operators that do not skip the clamp) have
+    zero derivative, which this backward does not mask: it raises instead."""
+
+    @staticmethod
+    def forward(ctx, E, x, op):  # noqa: D401
+        ctx.op = op
+        ctx.save_for_backward(x)
+        return op._apply(x, op.lambda_reg)
+
+    @staticmethod
+    def backward(ctx, gy):
+        op = ctx.op
+        (x,) = ctx.saved_tensors
+        gE = gx = None
+        if ctx.needs_input_grad[1]:
+            gx = op._apply(gy, op.lambda_reg).to(x.dtype)
+        if ctx.needs_input_grad[0]:
+            if not op.skip_clamp:
+                raise NotImplementedError(
+                    "embedding gradient of a clamped attention kernel is not implemented")
+            E = op.embeddings.detach()
+            X2 = x.detach().reshape(op.n, -1).to(op.dtype)
+            G2 = gy.detach().reshape(op.n, -1).to(op.dtype)
+            d = op.embedding_dim
+            gE = torch.zeros_like(E)
+            cols_per_chunk = max(1, 256 // (2 * d))  # right-hand sides per product
+            for c0 in range(0, X2.shape[1], cols_per_chunk):
+                c1 = min(c0 + cols_per_chunk, X2.shape[1])
+                xs, gs = X2[:, c0:c1], G2[:, c0:c1]  # (n, c)
+                R = torch.cat([(xs.unsqueeze(2) * E.unsqueeze(1)).reshape(op.n, -1),
+                               (gs.unsqueeze(2) * E.unsqueeze(1)).reshape(op.n, -1)], dim=1)
+                KR = op._apply(R.contiguous(), 0.0).reshape(op.n, 2, c1 - c0, d)
+                gE += (gs.unsqueeze(2) * KR[:, 0]).sum(dim=1) + (xs.unsqueeze(2) * KR[:, 1]).sum(dim=1)
+            gE = gE.to(op.embeddings.dtype)
+        return gE, gx, None
+
+
 class AttentionKernelOperator:
     """Matrix-free operator A = lambda*I + exp(E E^T) on the GPU.
 
@@ -122,31 +168,36 @@ class AttentionKernelOperator:
             0 if self.skip_clamp else 1,
         )
 
-    def _check_grad(self) -> None:
-        if self.embeddings.requires_grad and torch.is_grad_enabled():
-            raise NotImplementedError(
-                "autograd through the fused attention-kernel operator is not implemented"
-            )
-
     # -- KernelOperator protocol ---------------------------------------------
     def matvec(self, x: torch.Tensor) -> torch.Tensor:
-        """Apply (lambda I + G) to x of shape (n,) or (n, k)."""
+        """Apply (lambda I + G) to x of shape (n,) or (n, k).
+
+        Differentiable (laker/kernels.py:209-270 runs under autograd in the
+        reference's training code): with grad enabled and the embeddings or x
+        requiring grad, the product goes through _AttnMatvec, whose backward
+        runs on the same fused kernels."""
         if x.dim() not in (1, 2):
             raise ValueError(f"x must be 1-D or 2-D, got shape {x.shape}")
         if x.shape[0] != self.n:
             raise ValueError(f"x has {x.shape[0]} rows, operator has n={self.n}")
-        self._check_grad()
         _lib.require_cuda(x, "x")
         if self.n == 0:
             return torch.zeros_like(x)
+        if torch.is_grad_enabled() and (self.embeddings.requires_grad or x.requires_grad):
+            return _AttnMatvec.apply(self.embeddings, x, self)
+        return self._apply(x, self.lambda_reg)
+
+    def _apply(self, x: torch.Tensor, lam: float) -> torch.Tensor:
+        """(lam I + G) x on the fused kernels (no autograd)."""
         clamp = 0 if self.skip_clamp else 1
         p = self._packed
+        x = x.detach()
         if self.dtype == torch.float64:
             y = _lib.attn_matvec_f64(p.packed64, self.n, p.packed64, self.n, self.embedding_dim,
-                                     self.lambda_reg, clamp, x.to(torch.float64))
+                                     lam, clamp, x.to(torch.float64).contiguous())
         else:
             y = _lib.attn_matvec_f32(p.packed32, self.n, p.packed32, self.n, self.embedding_dim,
-                                     self.lambda_reg, clamp, x.to(torch.float32))
+                                     lam, clamp, x.to(torch.float32).contiguous())
         return y.to(x.dtype) if x.dtype in (torch.float32, torch.float64) else y
 
     def matvec_f64(self, x: torch.Tensor) -> torch.Tensor:
