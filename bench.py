@@ -439,8 +439,7 @@ def roofline_block(kernel_id, work, k1_avg_ms, achieved, exps_per_s, peaks, traf
     if kernel_id == 2:
         peak = peaks["mufu_tops"] * 1e12
         tf32 = work["entries"] * 96.0 / (k1_avg_ms * 1e-3) / 1e12
-        pk = _peaks_file()
-        tf32_peak = pk.get("bf16_tflops", 1590.0) / 2.0
+        tf32_peak, tf32_src = _tf32_peak()
         return dict(common, **{
             "bound": "mufu",
             "kernel": "k1t_matvec (symmetric FP32 operator, split-TF32 tcgen05 logits)",
@@ -449,7 +448,7 @@ def roofline_block(kernel_id, work, k1_avg_ms, achieved, exps_per_s, peaks, traf
             "peak_source": "MUFU ex2 microbenchmark measured in this run (laker_measure_peaks)",
             "fma_flops_per_launch": work["flops"], "fma_frac": achieved / peaks["ffma_tflops"],
             "tensor_tf32_tflops": tf32, "tensor_frac": tf32 / tf32_peak,
-            "tensor_peak_source": "half the measured cuBLAS bf16 burst (MEASURED_PEAKS.json): TF32 dense",
+            "tensor_peak_source": tf32_src,
         })
     return dict(common, **{
         "bound": "fma",
@@ -519,6 +518,17 @@ def count_reference_iterations(args) -> None:
 # ---------------------------------------------------------------------------
 # other workloads (one JSON line each; the default workload is the solve above)
 # ---------------------------------------------------------------------------
+def _tf32_peak() -> tuple:
+    """TF32 dense peak (TFLOP/s) and where it comes from: half the measured
+    cuBLAS bf16 burst of MEASURED_PEAKS.json, else half the pool's fallback
+    bf16 figure (1.59 PFLOP/s)."""
+    pk = _peaks_file()
+    if "bf16_tflops" in pk:
+        return pk["bf16_tflops"] / 2.0, ("half the measured cuBLAS bf16 burst (MEASURED_PEAKS.json): "
+                                        "TF32 dense rate, of measured")
+    return 1590.0 / 2.0, "half the fallback bf16 figure (1.59 PFLOP/s; MEASURED_PEAKS.json absent), of fallback"
+
+
 def _peaks_file() -> dict:
     try:
         return json.loads((REPO / "MEASURED_PEAKS.json").read_text())
@@ -566,10 +576,13 @@ def workload_fit(args) -> None:
     for _ in range(args.warmup):
         step()
     times = []
+    clocks = ClockSampler(dev)
+    clocks.start()
     for _ in range(args.steps):
         t0 = time.perf_counter()
         model, pred = step()
         times.append((time.perf_counter() - t0) * 1e3)
+    clocks.stop()
     ms = float(statistics.median(times))
     # float64 oracle with the same probes and FP32-computed embeddings
     E = model.embeddings.double().cpu().numpy()
@@ -588,6 +601,7 @@ def workload_fit(args) -> None:
     line["prediction_relerr_vs_float64_oracle"] = float(
         np.linalg.norm(pred.double().cpu().numpy() - pred_o) / np.linalg.norm(pred_o))
     line["relres_true"] = O.relres(E, LAMBDA, model.alpha.double().cpu().numpy(), y.double().numpy())
+    line["clocks"] = clocks.summary()
     line["cpu_baseline"] = {"value": 1.0 / cpu_s, "unit": "fits/s", "cores": O.c_threads(), "kind": "port",
                             "sample": f"float64 oracle fit + predict, full workload ({cpu_s:.2f} s, "
                                       f"{iters_o} PCG iterations)"}
@@ -654,8 +668,7 @@ def workload_variance(args) -> None:
     X = torch.randn(n, m, device=dev)
     k2_ms = _event_ms(lambda: op.matvec(X))
     tf32 = 3 * 2.0 * n * n * m / (k2_ms * 1e-3) / 1e12
-    pk = _peaks_file()
-    tf32_peak = pk.get("bf16_tflops", 1590.0) / 2.0
+    tf32_peak, tf32_src = _tf32_peak()
     # CPU: one 512-RHS float64 matvec on a row sample, x iterations
     import numpy as _np
     Eh = E.double().cpu().numpy()
@@ -678,8 +691,7 @@ def workload_variance(args) -> None:
         "roofline": {"bound": "tensor", "kernel": "k2_tc_matvec (tcgen05 kind::tf32, 3 split products)",
                      "achieved": tf32, "peak": tf32_peak, "unit": "TFLOP/s", "frac": tf32 / tf32_peak,
                      "traffic": None, "avg_launch_ms": k2_ms,
-                     "peak_source": "half of the measured cuBLAS bf16 burst (MEASURED_PEAKS.json): TF32 "
-                                    "dense rate"},
+                     "peak_source": tf32_src},
         "clocks": clocks.summary(),
         "cpu_baseline": {"value": cpu_rate, "unit": "queries/s", "cores": O.c_threads(), "kind": "port",
                          "sample": f"float64 oracle 512-RHS matvec on {rows} of {n} rows ({t_rows:.2f} s) "
@@ -782,9 +794,13 @@ def workload_serve(args) -> None:
         srv = Server(device=dev, hbm_budget=150e9)
         warm = make_trace(6, 1e4, seed=99, n_range=(1000, 4000), m_range=(16, 32))
         srv.run(warm)
+        clocks = ClockSampler(dev)
+        clocks.start()
         recs = srv.run(trace)
+        clocks.stop()
         s = summarize(recs)
         s["activity_s"] = dict(srv.stats)
+        s["clocks"] = clocks.summary()
         plain = run_plain(srv, trace)
         p = summarize(plain)
         out.append({"rate": rate, "served": s, "plain": p,
@@ -801,7 +817,7 @@ def workload_serve(args) -> None:
                                    "points) against a resident model, HBM budget 150 GB, tol 1e-6",
                        "rates": rates})
     line.update({"p50_ms": best["served"]["p50_ms"], "p99_ms": best["served"]["p99_ms"],
-                 "by_rate": out})
+                 "clocks": best["served"]["clocks"], "by_rate": out})
     print(json.dumps(line), flush=True)
 
 
