@@ -33,6 +33,7 @@
 // instance's arithmetic does not depend on where it sits or on the other
 // instances: the same bits alone or in any mix.
 #include <algorithm>
+#include <type_traits>
 #include <cstring>
 #include <vector>
 
@@ -265,28 +266,41 @@ __global__ void __launch_bounds__(BT)
       __syncthreads();
       const float4* V4 = reinterpret_cast<const float4*>(s_v);
       const double cis = si.cis;
-      for (int64_t i = c.row0 + warp; i < c.row1; i += NW) {
-        float s = 0.0f;
+      // rows of Q in groups of LPR lanes (8, 16 or 32 by the row's width):
+      // a warp takes 32 / LPR rows at a time and reduces within the group
+      auto rows = [&](auto lpr_tag) {
+        constexpr int LPR = decltype(lpr_tag)::value;
+        constexpr int RPW = 32 / LPR;
+        const int sub = lane / LPR, sl = lane % LPR;
+        for (int64_t i0 = c.row0 + (int64_t)warp * RPW; i0 < c.row1; i0 += (int64_t)NW * RPW) {
+          const int64_t i = i0 + sub;
+          float s = 0.0f;
+          if (i < c.row1) {
+            for (int c4 = sl; c4 < ldq4; c4 += LPR) {
+              const float4 q = __ldg(Q4 + i * ldq4 + c4);
+              const float4 vv = V4[c4];
+              s = fmaf(q.x, vv.x, s);
+              s = fmaf(q.y, vv.y, s);
+              s = fmaf(q.z, vv.z, s);
+              s = fmaf(q.w, vv.w, s);
+            }
+          }
 #pragma unroll
-        for (int ch = 0; ch < 8; ++ch) {
-          const int c4 = lane + 32 * ch;
-          if (c4 < ldq4) {
-            const float4 q = __ldg(Q4 + i * ldq4 + c4);
-            const float4 vv = V4[c4];
-            s = fmaf(q.x, vv.x, s);
-            s = fmaf(q.y, vv.y, s);
-            s = fmaf(q.z, vv.z, s);
-            s = fmaf(q.w, vv.w, s);
+          for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+          if (sl == 0 && i < c.row1) {
+            const double ri = r[c.seg + i];
+            const float zi = (float)(cis * ri + (double)s);
+            z[c.seg + i] = zi;
+            dot = fma(ri, (double)zi, dot);
           }
         }
-        s = warp_sum(s);
-        if (lane == 0) {
-          const double ri = r[c.seg + i];
-          const float zi = (float)(cis * ri + (double)s);
-          z[c.seg + i] = zi;
-          dot = fma(ri, (double)zi, dot);
-        }
-      }
+      };
+      if (ldq4 <= 64)
+        rows(std::integral_constant<int, 8>{});
+      else if (ldq4 <= 128)
+        rows(std::integral_constant<int, 16>{});
+      else
+        rows(std::integral_constant<int, 32>{});
     } else {
       for (int64_t i = c.row0 + tid; i < c.row1; i += BT) {
         const double ri = r[c.seg + i];
