@@ -15,6 +15,7 @@
 // residual.  Every kernel reads the device state first and does nothing once
 // the solve has finished, so the host can launch several iterations between
 // status polls.
+#include <cstdlib>
 #include "pcg_state.cuh"
 #include "sym.cuh"
 
@@ -308,6 +309,31 @@ struct PcgWs {
   size_t bytes;
 };
 
+// The captured iteration of a solve (released when the solve returns; a
+// graph still executing on the caller's stream is freed by the runtime once it
+// completes).
+struct IterGraph {
+  cudaStream_t cap = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  ~IterGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (cap) cudaStreamDestroy(cap);
+  }
+};
+
+// Whether laker_pcg_solve replays its iteration as a CUDA graph
+// (LAKER_PCG_GRAPH=0 launches the kernels one by one).
+bool pcg_use_graph() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("LAKER_PCG_GRAPH");
+    v = (e && e[0] == '0') ? 0 : 1;
+  }
+  return v == 1;
+}
+
 PcgWs carve(void* base, int64_t n, int d, int nr) {
   PcgWs w{};
   char* p = static_cast<char*>(base);
@@ -385,18 +411,18 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
   double* row64 = w.part64;
   double* col64 = sym_colpart_ptr<double>(w.part64, sp64);
   // r = b - A64 x (gated on the device by `gate`)
-  auto launch_residual = [&](int init, const int* gate) -> cudaError_t {
+  auto launch_residual = [&](int init, const int* gate, cudaStream_t cs) -> cudaError_t {
     cudaError_t ee;
     if (sym64) {
-      ee = launch_k4s(op->packed64, n, d, op->clamp, X, row64, col64, sp64, dstatus, gate, s);
+      ee = launch_k4s(op->packed64, n, d, op->clamp, X, row64, col64, sp64, dstatus, gate, cs);
       if (ee == cudaSuccess)
-        pcg_after_residual_kernel<true><<<G, T, 0, s>>>(nullptr, 0, sp64, row64, col64, B, X, w.r,
-                                                        n, init, w.blockpart, w.st);
+        pcg_after_residual_kernel<true><<<G, T, 0, cs>>>(nullptr, 0, sp64, row64, col64, B, X, w.r,
+                                                         n, init, w.blockpart, w.st);
     } else {
-      ee = launch_k4(op->packed64, n, op->packed64, n, d, op->clamp, X, w.part64, p4, dstatus, gate, s);
+      ee = launch_k4(op->packed64, n, op->packed64, n, d, op->clamp, X, w.part64, p4, dstatus, gate, cs);
       if (ee == cudaSuccess)
-        pcg_after_residual_kernel<false><<<G, T, 0, s>>>(w.part64, p4.S, sp64, nullptr, nullptr, B,
-                                                         X, w.r, n, init, w.blockpart, w.st);
+        pcg_after_residual_kernel<false><<<G, T, 0, cs>>>(w.part64, p4.S, sp64, nullptr, nullptr, B,
+                                                          X, w.r, n, init, w.blockpart, w.st);
     }
     return ee;
   };
@@ -419,17 +445,17 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
   LaunchTimer t32, t64;
   t32.init(prm->profile != 0);
   t64.init(prm->profile != 0);
-  auto launch_precond = [&](int init) {
+  auto launch_precond = [&](int init, cudaStream_t cs) {
     if (pc) {
       launch_precond_apply<float>(view, Gp, w.r, w.upart, w.v, w.z, w.blockpart,
                                   &w.st->counters[kCtrProject], &w.st->counters[kCtrExpand], w.st,
-                                  init, nullptr, &w.st->active, s);
+                                  init, nullptr, &w.st->active, cs);
       launches += 2;
     } else {
-      identity_expand_kernel<<<G, T, 0, s>>>(w.r, w.z, n, w.blockpart, w.st, init);
+      identity_expand_kernel<<<G, T, 0, cs>>>(w.r, w.z, n, w.blockpart, w.st, init);
       launches += 1;
     }
-    pcg_update_p_kernel<<<G, T, 0, s>>>(w.z, w.p, n, w.st, init);
+    pcg_update_p_kernel<<<G, T, 0, cs>>>(w.z, w.p, n, w.st, init);
     launches += 1;
   };
 
@@ -440,7 +466,7 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
   if (e != cudaSuccess) return fail_cuda(e);
   if (prm->has_x0) {
     // warm start: r = b - A x0 with the FP64 operator (laker/solvers.py:165-173)
-    e = launch_residual(1, nullptr);
+    e = launch_residual(1, nullptr, s);
     if (e != cudaSuccess) return fail_cuda(e);
     launches += 2;
   }
@@ -461,9 +487,55 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
     res->residual_norm = h.true_rnorm;
     return h.status;
   }
-  launch_precond(1);
+  launch_precond(1, s);
 
   // ---- iterations ----------------------------------------------------------
+  // One iteration: FP32 operator, alpha / x / r, the gated FP64 residual, the
+  // preconditioner and p.  Every decision is on the device (gates), so the
+  // iteration is launched as a CUDA graph captured once per solve (one graph
+  // launch instead of ~8 kernel launches per iteration); profiling runs launch
+  // the kernels directly so that the operator launches can be timed.
+  auto iteration = [&](cudaStream_t cs, bool timed) {
+    if (timed) t32.begin(cs);
+    if (tc) {
+      launch_k1t(w.img, n, op->clamp, w.p, sym_row, sym_col, sp, dstatus, &w.st->active, cs);
+    } else if (sym) {
+      launch_k1s(op->packed32, n, d, op->clamp, w.p, sym_row, sym_col, sp, dstatus, &w.st->active, cs);
+    } else {
+      launch_k1(op->packed32, n, op->packed32, n, d, op->clamp, w.p, w.part32, p1, dstatus,
+                &w.st->active, cs);
+    }
+    if (timed) t32.end(cs);
+    if (sym)
+      pcg_after_matvec_kernel<true><<<G, T, 0, cs>>>(w.part32, 0, sp, sym_row, sym_col, w.p, w.Ap, n,
+                                                     w.blockpart, w.st);
+    else
+      pcg_after_matvec_kernel<false><<<G, T, 0, cs>>>(w.part32, p1.S, sp, nullptr, nullptr, w.p, w.Ap,
+                                                      n, w.blockpart, w.st);
+    pcg_update_xr_kernel<<<G, T, 0, cs>>>(w.p, w.Ap, X, w.r, n, w.blockpart, w.st);
+    if (timed) t64.begin(cs);
+    launch_residual(0, &w.st->need_update, cs);
+    if (timed) t64.end(cs);
+    launches += 5;
+    launch_precond(0, cs);
+  };
+  IterGraph ig;
+  int iter_launches = 0;
+  if (prm->profile == 0 && pcg_use_graph()) {
+    const int before = launches;
+    e = cudaStreamCreateWithFlags(&ig.cap, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamBeginCapture(ig.cap, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      iteration(ig.cap, false);
+      const cudaError_t ce = cudaGetLastError();
+      e = cudaStreamEndCapture(ig.cap, &ig.graph);
+      if (e == cudaSuccess) e = ce;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&ig.exec, ig.graph, 0);
+    if (e != cudaSuccess) return fail_cuda(e);
+    iter_launches = launches - before;
+    launches = before;
+  }
   int check = prm->check_every;
   if (check < 1) {
     // poll roughly every 10 ms of FP32 operator work (~2e12 entries/s)
@@ -476,29 +548,13 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
   while (launched < prm->max_iter) {
     const int chunk = (prm->max_iter - launched) < check ? (prm->max_iter - launched) : check;
     for (int c = 0; c < chunk; ++c) {
-      t32.begin(s);
-      if (tc) {
-        launch_k1t(w.img, n, op->clamp, w.p, sym_row, sym_col, sp, dstatus, &w.st->active, s);
-      } else if (sym) {
-        launch_k1s(op->packed32, n, d, op->clamp, w.p, sym_row, sym_col, sp, dstatus,
-                   &w.st->active, s);
+      if (ig.exec) {
+        e = cudaGraphLaunch(ig.exec, s);
+        if (e != cudaSuccess) return fail_cuda(e);
+        launches += iter_launches;
       } else {
-        launch_k1(op->packed32, n, op->packed32, n, d, op->clamp, w.p, w.part32, p1, dstatus,
-                  &w.st->active, s);
+        iteration(s, true);
       }
-      t32.end(s);
-      if (sym)
-        pcg_after_matvec_kernel<true><<<G, T, 0, s>>>(w.part32, 0, sp, sym_row, sym_col, w.p, w.Ap, n,
-                                                      w.blockpart, w.st);
-      else
-        pcg_after_matvec_kernel<false><<<G, T, 0, s>>>(w.part32, p1.S, sp, nullptr, nullptr, w.p, w.Ap, n,
-                                                       w.blockpart, w.st);
-      pcg_update_xr_kernel<<<G, T, 0, s>>>(w.p, w.Ap, X, w.r, n, w.blockpart, w.st);
-      t64.begin(s);
-      launch_residual(0, &w.st->need_update);
-      t64.end(s);
-      launches += 5;
-      launch_precond(0);
     }
     launched += chunk;
     e = cudaGetLastError();
