@@ -21,6 +21,14 @@
 
 namespace laker {
 int precond_grid();
+// Grid of the preconditioner apply inside a solve: one CTA per 64 rows, at
+// most precond_grid() (small problems then do not leave most CTAs idle, and
+// the last CTA of the projection sums few partials).  Depends on n only.
+inline int precond_grid_for(int64_t n) {
+  const int64_t g = (n + 63) / 64;
+  const int cap = precond_grid();
+  return (int)(g < 1 ? 1 : (g > cap ? cap : g));
+}
 bool precond_valid(const laker_precond* pc);
 
 namespace {
@@ -404,7 +412,7 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
   const SymPlan sp = tc ? k1t_plan(n) : k1s_plan(n, d);
   double* sym_row = w.part32;
   float* sym_col = sym_colpart_ptr<float>(w.part32, sp);
-  const int G = vec_grid(n), Gp = precond_grid();
+  const int G = vec_grid(n), Gp = precond_grid_for(n);
   int* dstatus = &w.hdr->status;
   const bool sym64 = k4_use_symmetric();
   const SymPlan sp64 = k4s_plan(n, d);
