@@ -221,7 +221,8 @@ typedef struct laker_pcg_params {
   double tol;            /* stop when ||b - A x||_F <= tol ||b||_F (FP64 A)  */
   int max_iter;          /* iteration cap (reference default: n)           */
   double reliable_delta; /* FP64 residual recomputed when the recurrence
-                            residual fell by this factor (default 0.1)      */
+                            residual fell by this factor since the last
+                            recomputation (the Python solver passes 0.03)  */
   double breakdown_eps;  /* breakdown test p^T A p <= -eps ||p|| ||Ap||     */
   int check_every;       /* host polls the device status every N iterations */
   int has_x0;            /* 1: X holds the initial guess on entry           */
@@ -244,14 +245,21 @@ typedef struct laker_pcg_result {
 
 size_t laker_pcg_workspace_bytes(int64_t n, int d, int nr, int k);
 
-/* Solves A X = B for B (n x k, row-major, ld = k) with mixed-precision PCG:
+/* Solves A x = b (n right-hand-side values, k = 1) with mixed-precision PCG:
  * FP32 fused operator inside the iteration, FP64 vectors, inner products and
  * scalars on the device, and reliable updates that replace the recurrence
- * residual by the FP64 residual B - A X.  k = 1 is the single-RHS solve;
- * k > 1 uses column-wise alpha/beta and the global Frobenius stop test of the
- * batched-RHS solve.  `pc` may be NULL (identity preconditioner).
- * Replaces PreconditionedConjugateGradient.solve / solve_1d / solve_2d
- * (laker/solvers.py:130-394). */
+ * residual by the FP64 residual b - A x; the stop test is on that FP64
+ * residual.  k != 1 returns LAKER_ERR_UNSUPPORTED (the batched-RHS
+ * recurrence of solve_2d runs in the Python layer over
+ * laker_attn_matvec_f32 / _f64).  `pc` may be NULL (identity
+ * preconditioner).  Every decision of an iteration is taken on the device;
+ * the call captures one iteration as a CUDA graph on a private stream,
+ * replays it on `stream`, polls the device state every check_every
+ * iterations (0: about every 10 ms of work) and returns when the solve has
+ * ended (so it cannot itself be captured into a caller's graph).  With
+ * `profile` the kernels are launched one by one and the operator launches
+ * timed.  Replaces PreconditionedConjugateGradient.solve / solve_1d
+ * (laker/solvers.py:130-295). */
 int laker_pcg_solve(const laker_operator* op, const laker_precond* pc, const double* B, int k,
                     double* X, const laker_pcg_params* params, void* workspace,
                     size_t workspace_bytes, laker_pcg_result* result, void* stream);
