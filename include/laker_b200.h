@@ -109,13 +109,16 @@ int laker_attn_matvec_f32(const float* rows32, int64_t m, const float* cols32, i
  * No counterpart in the reference (roofline accounting). */
 int laker_fp32_matvec_work(int64_t n, int d, double* entries, double* flops, double* exps);
 
-/* Which kernel a square FP32 operator application of dimension d runs:
- * 0 the plain fused kernel, 1 the symmetric kernel with logits on the CUDA
- * cores, 2 the symmetric kernel with logits on the tensor cores (split-TF32
- * tcgen05 MMAs; then `flops` above counts only the CUDA-core accumulation
- * FMAs and the logits add 3 x 2 x 16 TF32 tensor flops per entry evaluated);
- * -1 for an invalid d.  No counterpart in the reference. */
-int laker_fp32_operator_kernel(int d);
+/* Which kernel a square FP32 operator application of n points of dimension
+ * d runs: 0 the plain fused kernel (always for n of at most
+ * LAKER_VARIANT_SYM_MIN_BLOCKS x 512 points, default 3072, where the
+ * symmetric kernels have too few block pairs to fill the GPU), 1 the
+ * symmetric kernel with logits on the CUDA cores, 2 the symmetric kernel with
+ * logits on the tensor cores (split-TF32 tcgen05 MMAs; then `flops` above
+ * counts only the CUDA-core accumulation FMAs and the logits add 3 x 2 x 16
+ * TF32 tensor flops per entry evaluated); -1 for invalid arguments.  No
+ * counterpart in the reference. */
+int laker_fp32_operator_kernel(int64_t n, int d);
 
 /* Kernel variant choices, changeable between calls (no call may be in flight
  * on any stream): they start from the environment switches and are what the
@@ -126,6 +129,10 @@ int laker_fp32_operator_kernel(int d);
  *   LAKER_VARIANT_K2_LOGITS_N128 of 33..128, and
  *   LAKER_VARIANT_K2_LOGITS_WIDE of more than 128: 0 logits on the CUDA cores
  *                                (default), 1 logits on the tensor cores
+ *   LAKER_VARIANT_SYM_MIN_BLOCKS square FP32 operators (single solves and
+ *                                matvecs; not the batched engine) of at most
+ *                                this many 512-point blocks take the plain
+ *                                kernel: 0..64, default 6
  * laker_set_variant returns the previous value, or -1 (nothing changed) for
  * an unknown `which` or an invalid value; laker_get_variant returns the
  * current value (-1 for an unknown `which`).  No counterpart in the
@@ -134,6 +141,7 @@ int laker_fp32_operator_kernel(int d);
 #define LAKER_VARIANT_K2_LOGITS_N32 1
 #define LAKER_VARIANT_K2_LOGITS_N128 2
 #define LAKER_VARIANT_K2_LOGITS_WIDE 3
+#define LAKER_VARIANT_SYM_MIN_BLOCKS 4
 int laker_set_variant(int which, int value);
 int laker_get_variant(int which);
 

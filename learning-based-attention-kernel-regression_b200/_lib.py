@@ -187,7 +187,7 @@ _SIGNATURES = {
         [c_int64, c_int, POINTER(c_double), POINTER(c_double), POINTER(c_double)],
     ),
     "laker_peaks_scratch_bytes": (c_size_t, []),
-    "laker_fp32_operator_kernel": (c_int, [c_int]),
+    "laker_fp32_operator_kernel": (c_int, [c_int64, c_int]),
     "laker_set_variant": (c_int, [c_int, c_int]),
     "laker_get_variant": (c_int, [c_int]),
     "laker_measure_peaks": (
@@ -427,6 +427,7 @@ VARIANT_K1T_UNIT = 0
 VARIANT_K2_LOGITS_N32 = 1
 VARIANT_K2_LOGITS_N128 = 2
 VARIANT_K2_LOGITS_WIDE = 3
+VARIANT_SYM_MIN_BLOCKS = 4
 
 
 def set_variant(which: int, value: int) -> int:
@@ -444,9 +445,9 @@ def get_variant(which: int) -> int:
     return v
 
 
-def fp32_operator_kernel(d: int) -> int:
+def fp32_operator_kernel(n: int, d: int) -> int:
     """0 plain, 1 symmetric (CUDA-core logits), 2 symmetric (tensor-core logits)."""
-    return int(load().laker_fp32_operator_kernel(d))
+    return int(load().laker_fp32_operator_kernel(n, d))
 
 
 def measure_peaks(device: torch.device) -> dict:

@@ -95,7 +95,7 @@ def autotune(n: int = 20000, d: int = 10, ks: Sequence[int] = (16, 64, 256), rep
         _lib.set_variant(which, best)
         out[name] = {"choice": best, "ms": times}
 
-    if _lib.fp32_operator_kernel(d) == 2:
+    if _lib.fp32_operator_kernel(n, d) == 2:
         x = torch.randn(n, generator=g).to(dev, torch.float32)
         pick("k1t_unit", _lib.VARIANT_K1T_UNIT, (4, 2), lambda: op.matvec(x))
     by_slot: Dict[int, int] = {}

@@ -491,7 +491,7 @@ extern "C" int laker_attn_matvec_f32(const float* rows32, int64_t m, const float
   // Single RHS: strided x is staged element-wise; a contiguous copy is not needed.
   if (ldx != 1) return LAKER_ERR_UNSUPPORTED;
   char* wbase = static_cast<char*>(workspace) + kWsHeader;
-  if (rows32 == cols32 && m == n && k1_use_symmetric()) {
+  if (rows32 == cols32 && m == n && k1_symmetric_for(n)) {
     // the operator itself: every off-diagonal entry evaluated once
     const bool tc = k1t_enabled(d);
     const SymPlan sp = tc ? k1t_plan(n) : k1s_plan(n, d);

@@ -731,6 +731,14 @@ cudaError_t launch_sym_finish64(const SymPlan& sp, const double* rowpart, const 
   return cudaGetLastError();
 }
 
+// Square operators of at most LAKER_VARIANT_SYM_MIN_BLOCKS 512-point blocks
+// (default 6: n <= 3072, at most 21 block pairs, so as many CTAs) run the
+// plain fused kernel, which spreads the rows over the whole GPU.
+bool k1_symmetric_for(int64_t n) {
+  const int64_t min_blocks = variant_get(LAKER_VARIANT_SYM_MIN_BLOCKS);
+  return k1_use_symmetric() && n > 0 && n > min_blocks * kSymRows * kSymThreads;
+}
+
 bool k1_use_symmetric() {
   static int v = -1;
   if (v < 0) {
@@ -758,7 +766,7 @@ extern "C" int laker_fp32_matvec_work(int64_t n, int d, double* entries, double*
   if (n < 0 || d < 1 || d > 16) return LAKER_ERR_INVALID_ARG;
   const double nn = (double)n * (double)n;
   double e, f;
-  if (k1_use_symmetric() && n > 0) {
+  if (k1_symmetric_for(n)) {
     // diagonal block pairs: every entry evaluated, used once (row sums);
     // off-diagonal pairs: evaluated once, used twice (row and column sums)
     const SymPlan sp = k1s_plan(n, d);
@@ -779,8 +787,8 @@ extern "C" int laker_fp32_matvec_work(int64_t n, int d, double* entries, double*
   return LAKER_OK;
 }
 
-extern "C" int laker_fp32_operator_kernel(int d) {
-  if (d < 1 || d > 16) return -1;
-  if (!k1_use_symmetric()) return 0;
+extern "C" int laker_fp32_operator_kernel(int64_t n, int d) {
+  if (n < 0 || d < 1 || d > 16) return -1;
+  if (!k1_symmetric_for(n)) return 0;
   return k1t_enabled(d) ? 2 : 1;
 }

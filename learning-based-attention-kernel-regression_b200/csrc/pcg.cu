@@ -407,7 +407,7 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   PcgWs w = carve(workspace, n, d, nr);
   const SegPlan p1 = k1_plan(n, n, d), p4 = k4_plan(n, n, d);
-  const bool sym = k1_use_symmetric();
+  const bool sym = k1_symmetric_for(n);
   const bool tc = sym && k1t_enabled(d);
   const SymPlan sp = tc ? k1t_plan(n) : k1s_plan(n, d);
   double* sym_row = w.part32;

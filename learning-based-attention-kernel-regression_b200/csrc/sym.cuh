@@ -153,6 +153,9 @@ cudaError_t launch_sym_finish(const SymPlan& sp, const double* rowpart, const fl
 // Whether square FP32 matvecs use the symmetric kernel (LAKER_K1_SYMMETRIC=0
 // selects the plain one, for comparisons).
 bool k1_use_symmetric();
+// Whether a square FP32 operator of n points takes the symmetric kernel
+// (k1_use_symmetric and more than LAKER_VARIANT_SYM_MIN_BLOCKS x 512 points).
+bool k1_symmetric_for(int64_t n);
 // Bytes of the symmetric partials: row sums (double), then column sums (CP:
 // float for the FP32 kernel, double for the FP64 one) at a 256-byte boundary.
 template <typename CP>

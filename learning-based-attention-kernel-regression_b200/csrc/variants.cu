@@ -10,13 +10,24 @@
 namespace laker {
 namespace {
 
-constexpr int kNumVariants = 4;
-std::atomic<int> g_variant[kNumVariants] = {{-1}, {-1}, {-1}, {-1}};
+constexpr int kNumVariants = 5;
+std::atomic<int> g_variant[kNumVariants] = {{-1}, {-1}, {-1}, {-1}, {-1}};
 
 int variant_default(int which) {
   if (which == LAKER_VARIANT_K1T_UNIT) {
     const char* e = getenv("LAKER_K1T_UNIT");
     return (e && e[0] == '2' && e[1] == 0) ? 2 : 4;
+  }
+  if (which == LAKER_VARIANT_SYM_MIN_BLOCKS) {
+    // Measured at n = 2000 (4 blocks): 16.2 us per launch for the plain
+    // kernel against 23.5 us for the tensor-core symmetric kernel, which then
+    // has 10 block pairs for 148 SMs; the two are equal at n = 5000.
+    const char* e = getenv("LAKER_SYM_MIN_BLOCKS");
+    if (e && e[0]) {
+      const int v = atoi(e);
+      if (v >= 0 && v <= 64) return v;
+    }
+    return 6;
   }
   const char* e = getenv("LAKER_K2_LOGITS_TC");
   return (e && e[0] == '1') ? 1 : 0;
@@ -24,6 +35,7 @@ int variant_default(int which) {
 
 bool variant_valid(int which, int value) {
   if (which == LAKER_VARIANT_K1T_UNIT) return value == 2 || value == 4;
+  if (which == LAKER_VARIANT_SYM_MIN_BLOCKS) return value >= 0 && value <= 64;
   return value == 0 || value == 1;
 }
 

@@ -52,10 +52,12 @@ def test_operator_kernel_query():
     from laker_b200 import _lib
 
     lib = _lib.load()
-    assert lib.laker_fp32_operator_kernel(10) in (0, 1, 2)
-    assert lib.laker_fp32_operator_kernel(16) == lib.laker_fp32_operator_kernel(10)
-    assert lib.laker_fp32_operator_kernel(0) == -1
-    assert lib.laker_fp32_operator_kernel(17) == -1
+    assert lib.laker_fp32_operator_kernel(100000, 10) in (1, 2)
+    assert lib.laker_fp32_operator_kernel(100000, 16) == lib.laker_fp32_operator_kernel(100000, 10)
+    assert lib.laker_fp32_operator_kernel(2000, 10) == 0  # small: the plain kernel
+    assert lib.laker_fp32_operator_kernel(100000, 0) == -1
+    assert lib.laker_fp32_operator_kernel(100000, 17) == -1
+    assert lib.laker_fp32_operator_kernel(-1, 10) == -1
 
 
 def test_variant_switches_without_gpu():
@@ -74,6 +76,14 @@ def test_variant_switches_without_gpu():
         assert lib.laker_set_variant(slot, 2) == -1
         assert lib.laker_set_variant(slot, 1 - v) == v
         assert lib.laker_set_variant(slot, v) == 1 - v
+    mb = lib.laker_get_variant(_lib.VARIANT_SYM_MIN_BLOCKS)
+    assert 0 <= mb <= 64
+    assert lib.laker_set_variant(_lib.VARIANT_SYM_MIN_BLOCKS, 65) == -1
+    assert lib.laker_set_variant(_lib.VARIANT_SYM_MIN_BLOCKS, 0) == mb
+    if lib.laker_fp32_operator_kernel(100000, 10) != 0:
+        assert lib.laker_fp32_operator_kernel(2000, 10) != 0  # forced symmetric
+        assert lib.laker_fp32_operator_kernel(0, 10) == 0
+    assert lib.laker_set_variant(_lib.VARIANT_SYM_MIN_BLOCKS, mb) == 0
     assert lib.laker_get_variant(9) == -1 and lib.laker_set_variant(9, 0) == -1
 
 

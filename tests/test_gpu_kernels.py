@@ -42,8 +42,24 @@ def test_matvec_golden(cuda, golden, key):
         assert rel(op.kernel_eval(q), g[f"{key}_keval"]) < max(tol, 1e-6 if dtype == torch.float32 else 0)
 
 
+@pytest.fixture(params=["default", "symmetric"])
+def sym_route(request):
+    """Run once with the default routing (small square operators on the plain
+    kernel) and once with the symmetric kernels forced down to one block."""
+    from laker_b200 import _lib
+
+    if request.param == "default":
+        yield request.param
+        return
+    prev = _lib.set_variant(_lib.VARIANT_SYM_MIN_BLOCKS, 0)
+    try:
+        yield request.param
+    finally:
+        _lib.set_variant(_lib.VARIANT_SYM_MIN_BLOCKS, prev)
+
+
 @pytest.mark.parametrize("n", [1, 2, 3, 255, 256, 257, 511, 513, 1029, 4097])
-def test_matvec_ragged_sizes(cuda, n):
+def test_matvec_ragged_sizes(cuda, n, sym_route):
     from laker_b200 import AttentionKernelOperator
 
     rng = np.random.default_rng(n)
@@ -184,7 +200,7 @@ def test_precond_apply_golden(cuda, golden):
     assert rel(pre.apply(V)[:, 1], pre.apply(v)) < 1e-5
 
 
-def test_pcg_fused_solves_to_tolerance(cuda, golden):
+def test_pcg_fused_solves_to_tolerance(cuda, golden, sym_route):
     from laker_b200 import AttentionKernelOperator, CCCPPreconditioner, PreconditionedConjugateGradient
 
     g = golden("solver_n400")
