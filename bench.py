@@ -12,6 +12,8 @@ Python API with y copied from pinned host memory and alpha read back.
 
 Multi-GPU: one process per GPU under torchrun; every rank solves its own
 instance (replicas, weak scaling); timing is the max over ranks.
+`--workload sharded` instead solves ONE system row-sharded over the ranks
+(strong scaling: p all-gathered over NCCL, three exchanges per iteration).
 `--impl reference` times the float64 CPU oracle of the reference path on the
 host cores (bounded sample, extrapolated) and prints the same JSON line.
 """
@@ -560,6 +562,143 @@ def _base_line(metric, value, unit, args, ms, dtype, config, higher=True):
             "vs_baseline": None, "dtype": dtype, "data": "synthetic", "config": config}
 
 
+def workload_sharded(args) -> None:
+    """One n-point solve row-sharded over the ranks (strong scaling).
+
+    Every rank builds the same system (seed 0) and the same CCCP factors, then
+    the ranks solve it together with sharded_pcg_solve: rows [r0, r1) of A p
+    per rank with the fused kernel, p all-gathered and the inner products
+    all-reduced over NCCL.  On one GPU the single shard holds every row and
+    takes the symmetric kernel, which shows the host-driven loop's cost against
+    the fused solve's CUDA-graph replay."""
+    import torch.distributed as dist
+
+    import laker_b200 as L
+    from laker_b200 import _lib
+    from laker_b200.distributed import ShardedPreconditioner, sharded_pcg_solve
+
+    rank, world, local = dist_info()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    n = args.n
+    op, pre, y = build_problem(n, seed=0, dev=dev)
+    dop = L.DistributedAttentionKernelOperator(op.embeddings, lambda_reg=op.lambda_reg)
+    ex, shard = dop.exchange, dop.shard
+    spre = ShardedPreconditioner.from_cccp(pre, ex.r0, ex.r1)
+    y_dev = y.to(dev)
+    peaks = _lib.measure_peaks(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def solve(b):
+        return sharded_pcg_solve(shard, ex, b, precond=spre, tol=TOL, max_iter=MAX_ITER)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        solve(y_dev)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    iters, accurate = [], []
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for i in range(args.steps):
+        flush.zero_()
+        ev[i][0].record()
+        x, info = solve(y_dev)
+        ev[i][1].record()
+        iters.append(info.iterations)
+        accurate.append(info.accurate_matvecs)
+    torch.cuda.synchronize()
+    barrier()
+    clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(step_ms)
+    relres = info.residual_norm / info.rhs_norm
+
+    y_host = y.clone().pin_memory()
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        xd, _ = solve(y_host.to(dev, non_blocking=True))
+        x_host = xd.to("cpu")
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_total = sum(e2e_ms)
+
+    # this rank's operator product alone, for the roofline
+    pf = torch.randn(n, device=dev, dtype=torch.float32)
+    k_ms = _event_ms(lambda: shard.apply32(pf, 0.0), reps=5)
+    if world > 1:
+        t = torch.tensor([total_ms, e2e_total, k_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, e2e_total, k_ms = (float(v) for v in t)
+    if rank == 0:
+        full = ex.rows == n
+        kernel_id = _lib.fp32_operator_kernel(n, EMBED_DIM) if full else 0
+        if full:
+            work = _lib.fp32_matvec_work(n, EMBED_DIM)
+        else:  # plain rectangular kernel over the largest shard: d + 1 FMAs and one exp2 per entry
+            ent = float(ex.chunk) * n
+            work = {"entries": ent, "flops": ent * 2.0 * (EMBED_DIM + 1), "exps": ent}
+        achieved = work["flops"] / (k_ms * 1e-3) / 1e12
+        roof = roofline_block(kernel_id, work, k_ms, achieved, work["exps"] / (k_ms * 1e-3), peaks,
+                              None, n, None)
+        roof["logical_entries_per_s"] = float(ex.chunk) * n / (k_ms * 1e-3)
+        roof["shard_rows"] = ex.chunk
+        # kernels of ours per solve: the operator (plain: k1 + finish; symmetric
+        # with tensor-core logits: pack + k1t + finish) per iteration and the
+        # FP64 residual (k4 + finish) per recomputation; vector updates are torch ops
+        per_op = 3 if kernel_id == 2 else 2
+        launches = sum(per_op * a + 2 * b for a, b in zip(iters, accurate))
+        line = {
+            "metric": METRIC + " (one system row-sharded over the GPUs)",
+            "value": args.steps / (total_ms / 1e3),
+            "unit": "solves/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "strong",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": {
+                "workload": f"exact-kernel PCG solve n={n} d={EMBED_DIM} N_r={NUM_PROBES} tol={TOL} "
+                            f"(true float64 residual), one system (seed 0) row-sharded over "
+                            f"{world} GPU(s)",
+                "n": n,
+                "parallelism": f"row shards x{world} (all_gather p, all_reduce scalars, NCCL)"
+                               if world > 1 else "single GPU, one shard (host-driven loop)",
+                "l2": "flushed between steps (256 MB write)",
+            },
+            "iterations": iters,
+            "fp64_residual_recomputations": accurate,
+            "relres_true": relres,
+            "p50_ms": float(np.percentile(step_ms, 50)),
+            "e2e": {"value": args.steps / (e2e_total / 1e3), "unit": "solves/s",
+                    "h2d_bytes_per_step": int(y_host.numel() * y_host.element_size()),
+                    "d2h_bytes_per_step": int(x_host.numel() * x_host.element_size())},
+            "roofline": roof,
+            "clocks": clocks.summary(),
+            "gpu_launches": int(launches),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def workload_fit(args) -> None:
     """Config: n=2000 fit + predict at 2000 points through LAKERRegressor."""
     import laker_b200 as L
@@ -838,10 +977,10 @@ def main() -> None:
     ap.add_argument("--count-reference-iterations", action="store_true")
     ap.add_argument("--kernel-only", action="store_true",
                     help="time the FP32 fused matvec alone (profiling target)")
-    ap.add_argument("--workload", choices=("solve", "fit", "variance", "batch", "serve"),
+    ap.add_argument("--workload", choices=("solve", "fit", "variance", "batch", "serve", "sharded"),
                     default="solve", help="solve: n=100k PCG solve (the default line); fit: n=2000 "
                     "fit+predict; variance: n=20k x 512 queries; batch: 1024 instances; serve: "
-                    "Poisson request trace")
+                    "Poisson request trace; sharded: one n=100k solve row-sharded over the GPUs")
     ap.add_argument("--rhs", type=int, default=1, help="--kernel-only: right-hand sides")
     ap.add_argument("--count", type=int, default=1024, help="batch: instances")
     ap.add_argument("--plain-subset", type=int, default=64, help="batch: single-path sample")
@@ -850,7 +989,7 @@ def main() -> None:
     args = ap.parse_args()
     if args.workload != "solve" and args.impl == "ours":
         {"fit": workload_fit, "variance": workload_variance, "batch": workload_batch,
-         "serve": workload_serve}[args.workload](args)
+         "serve": workload_serve, "sharded": workload_sharded}[args.workload](args)
         return
     if args.warmup < 3 and args.impl == "ours" and not args.kernel_only:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

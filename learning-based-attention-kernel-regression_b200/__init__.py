@@ -23,6 +23,7 @@ from .core import LAKERCore
 from .data import batch_instances, synthetic_field
 from .embeddings import PositionEmbedding
 from .kernels import AttentionKernelOperator, KernelOperator
+from .distributed import DistributedAttentionKernelOperator, sharded_pcg_solve
 from .models import LAKERRegressor
 from .preconditioner import CCCPPreconditioner, adaptive_shrinkage_rho, eigh_stable
 from .solvers import PreconditionedConjugateGradient
@@ -46,6 +47,7 @@ __all__ = [
     "BatchedPCG",
     "build_cccp_batched",
     "CCCPPreconditioner",
+    "DistributedAttentionKernelOperator",
     "EngineCapacityError",
     "SolveEngine",
     "engine_bytes_per_instance",
@@ -58,6 +60,7 @@ __all__ = [
     "adaptive_shrinkage_rho",
     "batch_instances",
     "build",
+    "sharded_pcg_solve",
     "eigh_stable",
     "get_default_device",
     "get_default_dtype",

@@ -24,6 +24,7 @@ import torch.nn as nn
 from . import _lib
 from .backend import get_default_device, get_default_dtype
 from .embeddings import PositionEmbedding
+from .distributed import DistributedAttentionKernelOperator
 from .kernels import AttentionKernelOperator, KernelOperator
 from .preconditioner import CCCPPreconditioner
 from .solvers import PreconditionedConjugateGradient
@@ -133,9 +134,15 @@ class LAKERCore:
             raise NotImplementedError(
                 f"kernel_approx={self.kernel_approx!r} is outside the B200 exact-kernel path"
             )
-        if self.distributed:
-            raise NotImplementedError("the multi-device operator is outside the B200 path")
         lam = float(lambda_reg) if lambda_reg is not None else self.lambda_reg
+        if self.distributed:
+            # rows sharded over the ranks of the default process group (one
+            # process per GPU); a single device when there is no group
+            op = DistributedAttentionKernelOperator(embeddings=embeddings, lambda_reg=lam,
+                                                    master_device=self.device, dtype=self.dtype)
+            if self.verbose:
+                logger.info("Using distributed kernel on %d device(s)", len(op.devices))
+            return op
         n = embeddings.shape[0]
         chunk = chunk_size
         if chunk is None and n > 5000:

@@ -26,6 +26,8 @@ from typing import Callable, Optional
 import torch
 
 from . import _lib
+from .distributed import (DistributedAttentionKernelOperator, ShardedPreconditioner,
+                          ShardedSolveInfo, sharded_pcg_solve)
 from .kernels import AttentionKernelOperator
 from .preconditioner import CCCPPreconditioner
 
@@ -110,6 +112,9 @@ class PreconditionedConjugateGradient:
             pc = _bound_self(preconditioner, CCCPPreconditioner, ("apply", "apply_1d", "apply_impl"))
             fused_pc = pc is not None
         if op is not None and fused_pc and not self.autograd_safe and self.restart_freq is None:
+            if rhs.dim() == 1 and isinstance(op, DistributedAttentionKernelOperator) \
+                    and not op.single_device:
+                return self._solve_sharded(op, pc, rhs, x0, max_iter)
             if rhs.dim() == 1:
                 return self._solve_fused(op, pc, rhs, x0, max_iter)
             return self._solve_mixed_2d(op, preconditioner, rhs, x0, max_iter)
@@ -153,6 +158,29 @@ class PreconditionedConjugateGradient:
         if res.rhs_norm == 0.0:
             return x.to(rhs.dtype)
         self._finish(res.status, res.residual_norm / res.rhs_norm)
+        return x.to(rhs.dtype)
+
+    def _solve_sharded(self, op: DistributedAttentionKernelOperator,
+                       pc: Optional[CCCPPreconditioner], rhs: torch.Tensor,
+                       x0: Optional[torch.Tensor], max_iter: int) -> torch.Tensor:
+        """Row-sharded solve over the operator's process group (every rank
+        calls it with the same rhs and gets the full solution)."""
+        e = op.exchange
+        pre = ShardedPreconditioner.from_cccp(pc, e.r0, e.r1) if pc is not None else None
+        info = ShardedSolveInfo()
+        try:
+            x, _ = sharded_pcg_solve(op.shard, e, rhs, precond=pre, x0=x0, tol=self.tol,
+                                     max_iter=max_iter, reliable_delta=self.reliable_delta,
+                                     breakdown_eps=self._eps(rhs.dtype), info=info)
+        finally:
+            self.iterations = info.iterations
+            self.accurate_matvecs = info.accurate_matvecs
+            self.residual_norm = info.residual_norm
+            self.rhs_norm = info.rhs_norm
+            self.recurrence_norm = info.recurrence_norm
+            self.status = info.status
+        if info.rhs_norm > 0.0:
+            self._finish(info.status, info.residual_norm / info.rhs_norm)
         return x.to(rhs.dtype)
 
     def _solve_mixed_2d(self, op: AttentionKernelOperator, preconditioner, rhs, x0, max_iter):
