@@ -9,13 +9,15 @@ Public API (drop-in for the solve path of the `laker` package):
     LAKERCore / LAKERRegressor  laker.core / laker.models
 
 The heavy lifting is in liblaker_b200.so (C ABI: include/laker_b200.h), built
-in-tree by `laker_b200.build()`.  Every operator requires CUDA tensors; there
+in-tree by `laker_b200.build()`; its entry points are registered as torch
+custom ops (`torch.ops.laker_b200.*`, module `laker_b200.ops`), which the
+classes above call.  Every operator requires CUDA tensors; there
 is no CPU implementation to fall back on.
 """
 
 from __future__ import annotations
 
-from . import _lib
+from . import _lib, ops
 from ._build import LIB_PATH
 from ._build import build as _build_lib
 from .backend import get_default_device, get_default_dtype, set_default_device, set_default_dtype

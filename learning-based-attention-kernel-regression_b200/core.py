@@ -21,7 +21,7 @@ from typing import Optional, Tuple, Union
 import torch
 import torch.nn as nn
 
-from . import _lib
+from . import _lib, ops
 from .backend import get_default_device, get_default_dtype
 from .embeddings import PositionEmbedding
 from .distributed import DistributedAttentionKernelOperator
@@ -208,9 +208,9 @@ class LAKERCore:
         clamp = 0
         if not op.skip_clamp or (m and torch.sum(q.double() ** 2, dim=1).max().item() >= 700.0):
             clamp = 1
-        q64 = _lib.pack_f64(q)
-        out = _lib.attn_matvec_f64(q64, m, op.packed.packed64, op.n, op.embedding_dim, 0.0, clamp,
-                                   alpha.to(torch.float64))
+        q64 = ops.pack(q, 64)
+        out = ops.attn_matvec(q64, m, op.packed.packed64, op.n, op.embedding_dim, 0.0, bool(clamp),
+                              alpha)
         out = out.to(self.dtype)
         if residual_corrector is not None:
             residual_corrector.eval()
@@ -235,10 +235,10 @@ class LAKERCore:
         for start in range(0, m, VARIANCE_BLOCK):
             end = min(start + VARIANCE_BLOCK, m)
             qb = q[start:end]
-            q64 = _lib.pack_f64(qb)
-            kxq = _lib.kernel_eval(op.packed.packed64, op.n, q64, end - start, d,
-                                   0 if op.skip_clamp else 1, torch.float64, q.device)
+            q64 = ops.pack(qb, 64)
+            kxq = ops.kernel_eval(op.packed.packed64, op.n, q64, end - start, d, not op.skip_clamp,
+                                  True)
             v = pcg.solve(op.matvec, preconditioner.apply, kxq)
-            var[start:end] = _lib.variance_finalize(q64, end - start, d, kxq, v.to(torch.float64))
+            var[start:end] = ops.variance_finalize(q64, end - start, d, kxq, v)
         self.last_pcg = pcg
         return var.to(self.dtype)

@@ -39,7 +39,7 @@ from typing import List, Optional, Tuple
 import torch
 import torch.distributed as dist
 
-from . import _lib
+from . import _lib, ops
 from .kernels import AttentionKernelOperator
 from .preconditioner import CCCPPreconditioner
 
@@ -128,7 +128,7 @@ class RowShard:
             self.rows32, self.rows64 = self.cols32, self.cols64
         elif self.rows > 0:
             E = op.embeddings.detach()[r0:r1]
-            self.rows32, self.rows64 = _lib.pack_f32(E), _lib.pack_f64(E)
+            self.rows32, self.rows64 = ops.pack(E, 32), ops.pack(E, 64)
 
     def _local(self, full: torch.Tensor) -> torch.Tensor:
         return full[self.r0: self.r1]
@@ -138,8 +138,8 @@ class RowShard:
         if self.rows == 0:
             return xf.new_zeros((0,) + tuple(xf.shape[1:]), dtype=torch.float32)
         xf = xf.to(torch.float32).contiguous()
-        y = _lib.attn_matvec_f32(self.rows32, self.rows, self.cols32, self.n, self.d, 0.0,
-                                 self.clamp, xf)
+        y = ops.attn_matvec(self.rows32, self.rows, self.cols32, self.n, self.d, 0.0,
+                            bool(self.clamp), xf)
         return y.add_(self._local(xf), alpha=lam) if lam != 0.0 else y
 
     def apply64(self, xf: torch.Tensor, lam: float) -> torch.Tensor:
@@ -147,8 +147,8 @@ class RowShard:
         if self.rows == 0:
             return xf.new_zeros((0,) + tuple(xf.shape[1:]), dtype=torch.float64)
         xf = xf.to(torch.float64).contiguous()
-        y = _lib.attn_matvec_f64(self.rows64, self.rows, self.cols64, self.n, self.d, 0.0,
-                                 self.clamp, xf)
+        y = ops.attn_matvec(self.rows64, self.rows, self.cols64, self.n, self.d, 0.0,
+                            bool(self.clamp), xf)
         return y.add_(self._local(xf), alpha=lam) if lam != 0.0 else y
 
     def residual64(self, xf: torch.Tensor, b_loc: torch.Tensor) -> torch.Tensor:
@@ -156,8 +156,8 @@ class RowShard:
         if self.rows == 0:
             return b_loc.to(torch.float64).clone()
         xf = xf.to(torch.float64).contiguous()
-        r = _lib.attn_matvec_f64(self.rows64, self.rows, self.cols64, self.n, self.d, 0.0,
-                                 self.clamp, xf, B=b_loc.to(torch.float64).contiguous())
+        r = ops.attn_residual(self.rows64, self.rows, self.cols64, self.n, self.d, 0.0,
+                              bool(self.clamp), xf, b_loc)
         return r.sub_(self._local(xf), alpha=self.lam)
 
 

@@ -16,7 +16,7 @@ from typing import Optional, Protocol, Tuple
 
 import torch
 
-from . import _lib
+from . import _lib, ops
 
 logger = logging.getLogger(__name__)
 
@@ -62,8 +62,8 @@ class PackedEmbeddings:
                 f"got {E.shape[1]}"
             )
         self.n, self.d = int(E.shape[0]), int(E.shape[1])
-        self.packed32 = _lib.pack_f32(E.detach())
-        self.packed64 = _lib.pack_f64(E.detach())
+        self.packed32 = ops.pack(E.detach(), 32)
+        self.packed64 = ops.pack(E.detach(), 64)
 
 
 class _AttnMatvec(torch.autograd.Function):
@@ -189,44 +189,37 @@ class AttentionKernelOperator:
 
     def _apply(self, x: torch.Tensor, lam: float) -> torch.Tensor:
         """(lam I + G) x on the fused kernels (no autograd)."""
-        clamp = 0 if self.skip_clamp else 1
         p = self._packed
         x = x.detach()
-        if self.dtype == torch.float64:
-            y = _lib.attn_matvec_f64(p.packed64, self.n, p.packed64, self.n, self.embedding_dim,
-                                     lam, clamp, x.to(torch.float64).contiguous())
-        else:
-            y = _lib.attn_matvec_f32(p.packed32, self.n, p.packed32, self.n, self.embedding_dim,
-                                     lam, clamp, x.to(torch.float32).contiguous())
+        packed = p.packed64 if self.dtype == torch.float64 else p.packed32
+        y = ops.attn_matvec(packed, self.n, packed, self.n, self.embedding_dim, lam,
+                            not self.skip_clamp, x)
         return y.to(x.dtype) if x.dtype in (torch.float32, torch.float64) else y
 
     def matvec_f64(self, x: torch.Tensor) -> torch.Tensor:
         """FP64 (accurate) application regardless of the operator dtype."""
         _lib.require_cuda(x, "x")
         p = self._packed
-        return _lib.attn_matvec_f64(p.packed64, self.n, p.packed64, self.n, self.embedding_dim,
-                                    self.lambda_reg, 0 if self.skip_clamp else 1,
-                                    x.to(torch.float64))
+        return ops.attn_matvec(p.packed64, self.n, p.packed64, self.n, self.embedding_dim,
+                               self.lambda_reg, not self.skip_clamp, x)
 
     def residual_f64(self, x: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
         """b - A x with the FP64 operator."""
         _lib.require_cuda(x, "x")
         p = self._packed
-        return _lib.attn_matvec_f64(p.packed64, self.n, p.packed64, self.n, self.embedding_dim,
-                                    self.lambda_reg, 0 if self.skip_clamp else 1,
-                                    x.to(torch.float64), B=b.to(torch.float64))
+        return ops.attn_residual(p.packed64, self.n, p.packed64, self.n, self.embedding_dim,
+                                 self.lambda_reg, not self.skip_clamp, x, b)
 
     def diagonal(self) -> torch.Tensor:
         """diag(lambda I + G) = lambda + exp(||e_i||^2)."""
-        d = _lib.attn_diagonal(self._packed.packed64, self.n, self.embedding_dim, self.lambda_reg,
-                               self.device)
+        d = ops.attn_diagonal(self._packed.packed64, self.n, self.embedding_dim, self.lambda_reg)
         return d.to(self.dtype)
 
     def to_dense(self) -> torch.Tensor:
         """Materialise lambda I + G (O(n^2) memory: small n only)."""
         p = self._packed
-        g = _lib.kernel_eval(p.packed64, self.n, p.packed64, self.n, self.embedding_dim, 0,
-                             self.dtype, self.device)
+        g = ops.kernel_eval(p.packed64, self.n, p.packed64, self.n, self.embedding_dim, False,
+                            self.dtype == torch.float64)
         g.diagonal().add_(self.lambda_reg)
         return g
 
@@ -244,7 +237,7 @@ class AttentionKernelOperator:
             if y.dim() != 2 or y.shape[1] != x.shape[1]:
                 raise ValueError(f"y must be 2-D with {x.shape[1]} columns, got {tuple(y.shape)}")
             _lib.require_cuda(y, "y")
-            cols64, p = _lib.pack_f64(y.to(self.dtype)), y.shape[0]
-        rows64 = _lib.pack_f64(x.to(self.dtype))
-        return _lib.kernel_eval(rows64, x.shape[0], cols64, p, x.shape[1],
-                                0 if self.skip_clamp else 1, self.dtype, self.device)
+            cols64, p = ops.pack(y.to(self.dtype), 64), y.shape[0]
+        rows64 = ops.pack(x.to(self.dtype), 64)
+        return ops.kernel_eval(rows64, x.shape[0], cols64, p, x.shape[1], not self.skip_clamp,
+                               self.dtype == torch.float64)

@@ -24,7 +24,7 @@ from typing import Callable, Optional
 
 import torch
 
-from . import _lib
+from . import _lib, ops
 from .backend import get_default_device, get_default_dtype
 
 logger = logging.getLogger(__name__)
@@ -352,7 +352,9 @@ class CCCPPreconditioner:
 
     def apply_1d(self, x: torch.Tensor) -> torch.Tensor:
         _lib.require_cuda(x, "x")
-        return _lib.precond_apply(self.c_precond(), x, x.dtype)
+        self.c_precond()  # raises before the first build
+        return ops.precond_apply(self._q32, self._w32, self.n, self.nr,
+                                 self.isotropic_coef ** (-0.5), x, x.dtype == torch.float64)
 
     def apply_2d(self, x: torch.Tensor) -> torch.Tensor:
         _lib.require_cuda(x, "x")

@@ -25,7 +25,7 @@ from typing import Callable, Optional
 
 import torch
 
-from . import _lib
+from . import _lib, ops
 from .distributed import (DistributedAttentionKernelOperator, ShardedPreconditioner,
                           ShardedSolveInfo, sharded_pcg_solve)
 from .kernels import AttentionKernelOperator
@@ -137,17 +137,17 @@ class PreconditionedConjugateGradient:
 
     def _solve_fused(self, op: AttentionKernelOperator, pc: Optional[CCCPPreconditioner],
                      rhs: torch.Tensor, x0: Optional[torch.Tensor], max_iter: int) -> torch.Tensor:
-        b = rhs.to(torch.float64).contiguous()
-        if x0 is not None:
-            x = x0.to(device=rhs.device, dtype=torch.float64).clone().contiguous()
-        else:
-            x = torch.empty_like(b)
-        params = _lib.laker_pcg_params(
-            self.tol, int(max_iter), self.reliable_delta, self._eps(rhs.dtype), self.check_every,
-            int(x0 is not None), int(self.profile),
-        )
-        res = _lib.pcg_solve(op.c_operator(), pc.c_precond() if pc is not None else None, b, x,
-                             params)
+        p = op.packed
+        if pc is not None:
+            pc.c_precond()  # raises before the first build
+        x, stats = ops.pcg_solve(
+            p.packed32, p.packed64, op.n, op.embedding_dim, op.lambda_reg, not op.skip_clamp,
+            pc._q32 if pc is not None else None, pc._w32 if pc is not None else None,
+            pc.nr if pc is not None else 0,
+            pc.isotropic_coef ** (-0.5) if pc is not None else 0.0, rhs, x0, self.tol,
+            int(max_iter), self.reliable_delta, self._eps(rhs.dtype), self.check_every,
+            self.profile)
+        res = ops.result_from_stats(stats)
         self.last_result = res
         self.iterations = int(res.iterations)
         self.accurate_matvecs = int(res.accurate_matvecs)
