@@ -129,6 +129,12 @@ int laker_fp32_operator_kernel(int64_t n, int d);
  *   LAKER_VARIANT_K2_LOGITS_N128 of 33..128, and
  *   LAKER_VARIANT_K2_LOGITS_WIDE of more than 128: 0 logits on the CUDA cores
  *                                (default), 1 logits on the tensor cores
+ *   LAKER_VARIANT_K1T_LOGITS     operands of the tensor-core symmetric
+ *                                operator's logits: 0 split TF32, 1 split
+ *                                FP16 (default; three kind::f16 products of
+ *                                K = 16; unclamped operators only, clamped
+ *                                ones keep split TF32).  An engine keeps the
+ *                                format it was initialised with.
  *   LAKER_VARIANT_SYM_MIN_BLOCKS square FP32 operators (single solves and
  *                                matvecs; not the batched engine) of at most
  *                                this many 512-point blocks take the plain
@@ -142,6 +148,7 @@ int laker_fp32_operator_kernel(int64_t n, int d);
 #define LAKER_VARIANT_K2_LOGITS_N128 2
 #define LAKER_VARIANT_K2_LOGITS_WIDE 3
 #define LAKER_VARIANT_SYM_MIN_BLOCKS 4
+#define LAKER_VARIANT_K1T_LOGITS 5
 int laker_set_variant(int which, int value);
 int laker_get_variant(int which);
 

@@ -428,6 +428,7 @@ VARIANT_K2_LOGITS_N32 = 1
 VARIANT_K2_LOGITS_N128 = 2
 VARIANT_K2_LOGITS_WIDE = 3
 VARIANT_SYM_MIN_BLOCKS = 4
+VARIANT_K1T_LOGITS = 5
 
 
 def set_variant(which: int, value: int) -> int:

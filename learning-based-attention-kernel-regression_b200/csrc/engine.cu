@@ -528,6 +528,7 @@ struct EngineLayout {
   int64_t cap_points = 0, cap_blocks = 0, cap_pairs = 0;
   int slots = 0, ustride = 4, dp = 2;
   bool tc = false;  // FP32 operator on the tensor cores (operand image arena)
+  int fmt = 0;      // its image format (k1t_format at init), for every pack and launch
   size_t bytes = 0;
   size_t o_img = 0;
   size_t o_hdr, o_slots, o_st, o_done, o_ctr, o_scal, o_acti, o_actp, o_needi, o_needp, o_vvec,
@@ -578,6 +579,7 @@ EngineLayout engine_layout(const laker_engine_config& cfg) {
   L.o_row64 = take(PP * 8);
   L.o_col64 = take(PP * 8);
   L.tc = k1t_enabled(cfg.d);
+  L.fmt = k1t_format(cfg.clamp);
   if (L.tc) L.o_img = take(k1t_image_bytes(L.cap_points));
   L.bytes = o;
   return L;
@@ -650,7 +652,7 @@ cudaError_t engine_iteration(EngineHost* e, cudaStream_t cs) {
   int* scal = e->at<int>(L.o_scal);
   cudaError_t err =
       L.tc ? launch_k1t_batched(e->at<uint8_t>(L.o_img), clamp, p, row32, col32, e->sp32, e->bm32,
-                                status, ed.active, cs)
+                                status, ed.active, cs, L.fmt)
            : launch_k1s_batched(e->at<float>(L.o_p32), d, clamp, p, row32, col32, e->sp32, e->bm32,
                                 status, ed.active, cs);
   if (err != cudaSuccess) return err;
@@ -691,7 +693,7 @@ cudaError_t pack_slot_image(EngineHost* e, const SlotInfo& si) {
   if (!L.tc) return cudaSuccess;
   return launch_k1t_pack(e->at<float>(L.o_p32) + (size_t)si.seg * L.dp, si.npts, e->cfg.d,
                          e->at<uint8_t>(L.o_img) + (size_t)si.blk_start * k1t_image_bytes(1),
-                         si.nblk * RB, e->stream);
+                         si.nblk * RB, e->stream, L.fmt);
 }
 
 // Re-places a slot's record and block map (device) from its host record.

@@ -23,6 +23,13 @@
 // K-major layout the tensor core reads: rows scaled by log2 e (hi, lo), then
 // columns unscaled (hi, lo).  One bulk copy brings a block's row operands
 // (64 KB), one its column operands (64 KB).
+// FP16 format (unclamped operators, LAKER_VARIANT_K1T_LOGITS = 1): six
+// variants of 32 bytes (16 FP16) per point in the 32-byte-swizzled K-major
+// layout, rows scaled by log2 e (H, L, Hs), then columns (H, L, Hs), with
+// H = fp16(v), L = fp16((v - H) 2^12), Hs = fp16(H 2^-12); the logits are
+// H H' + Hs L' + L Hs' (= H H' + H lo' + lo H'), three kind::f16 MMAs of K =
+// 16 per row tile instead of six kind::tf32 MMAs of K = 8, half the operand
+// bytes (48 KB per side) and the f16 tensor rate.
 //
 // Roles in a CTA of 576 threads (one CTA per SM: 512 TMEM columns, up to
 // 221 KB of shared memory), no CTA-wide barrier in the main loop:
@@ -41,6 +48,8 @@
 // checks; the CTA then drains its copies and MMAs and frees TMEM.  The
 // epilogue warps keep walking their pairs after an abort (without waits or
 // TMEM reads) so that their named barriers always match.
+#include <cuda_fp16.h>
+
 #include <cstdlib>
 
 #include "sym.cuh"
@@ -65,23 +74,31 @@ constexpr int kTCopyWarp = kTEpi / 32, kTMmaWarp = kTEpi / 32 + 1;
 constexpr int kTNcg = 4;                       // column groups (warps per row quadrant)
 constexpr int kTCW = kTSlabN / kTNcg;          // columns per warp per slab (16)
 static_assert(kTB == 512, "the finish and the engine use 512-point blocks");
+// FP16 image format
+constexpr uint32_t kTRowBytes16 = 32;              // 16 FP16 per point
+constexpr uint32_t kTVar16 = kTB * kTRowBytes16;   // one FP16 variant of a block (16 KB)
+constexpr uint32_t kTHalf16 = 3 * kTVar16;         // H, L, Hs of one side (48 KB)
+constexpr uint32_t kTSBO16 = 8 * kTRowBytes16;     // 8-row core group
+constexpr uint32_t kTLayout16 = 6;                 // SWIZZLE_32B
+static_assert(2 * kTHalf16 <= kTImgBlock, "the FP16 image fits the block's 128 KB");
 
 // Plan for TMEM units of UT row tiles (UT x 64 accumulator columns, 512 / (64
 // UT) buffers): UT = 4 holds a whole slab per buffer (2 buffers), UT = 2 half
 // a slab (4 buffers, more MMA look-ahead, twice the handshakes).  Offsets are
 // from a 1024-byte aligned base.
-template <int UT>
+template <int UT, int FMT>
 struct K1tCfg {
   static_assert(UT == 2 || UT == 4, "row tiles per unit");
   static constexpr int kBufs = 8 / UT;
+  static constexpr uint32_t kHalf = FMT == kK1tF16 ? kTHalf16 : kTHalf;  // one side of a block
   // mbarrier slots: row operands full / empty, column stages full [2] /
   // empty [2], TMEM buffers full [kBufs] / empty [kBufs], MMA drain
   static constexpr int kBarAFull = 0, kBarAEmpty = 1, kBarBFull = 2, kBarBEmpty = 4,
                        kBarAccFull = 6, kBarAccEmpty = kBarAccFull + kBufs,
                        kBarDrain = kBarAccEmpty + kBufs, kNumBars = kBarDrain + 1;
   static constexpr uint32_t kOffA = 0;                        // row operands (hi | lo)
-  static constexpr uint32_t kOffB = kOffA + kTHalf;           // 2 stages of column operands
-  static constexpr uint32_t kOffXb = kOffB + 2 * kTHalf;      // 2 x 512 floats: x of the column block
+  static constexpr uint32_t kOffB = kOffA + kHalf;            // 2 stages of column operands
+  static constexpr uint32_t kOffXb = kOffB + 2 * kHalf;       // 2 x 512 floats: x of the column block
   static constexpr uint32_t kOffRow = kOffXb + 2 * kTB * 4;   // 4 x 512 doubles: row sums per column group
   static constexpr uint32_t kOffCol = kOffRow + kTNcg * kTB * 8;  // 4 x 512 floats: column sums per row quadrant
   static constexpr uint32_t kOffBar = kOffCol + 4 * kTB * 4;  // barriers, TMEM slot, abort flag
@@ -93,6 +110,51 @@ struct K1tCfg {
 // (64-byte swizzle: 16-byte chunk index XOR bits 1-2 of the row).
 __host__ __device__ inline uint32_t k1t_offset(uint32_t r, uint32_t k) {
   return r * kTRowBytes + ((((k >> 2) ^ ((r >> 1) & 3u)) << 4)) + (k & 3u) * 4u;
+}
+
+// Byte offset of FP16 element k of point row r inside an FP16 block variant
+// (32-byte swizzle: 16-byte chunk index XOR bit 2 of the row).
+__host__ __device__ inline uint32_t k1t16_offset(uint32_t r, uint32_t k) {
+  return r * kTRowBytes16 + ((((k >> 3) ^ ((r >> 2) & 1u)) << 4)) + (k & 7u) * 2u;
+}
+
+__device__ __forceinline__ void split_f16(float v, uint16_t& h, uint16_t& l, uint16_t& hs) {
+  const __half hh = __float2half_rn(v);
+  const float hf = __half2float(hh);
+  h = __half_as_ushort(hh);
+  l = __half_as_ushort(__float2half_rn((v - hf) * 4096.0f));
+  hs = __half_as_ushort(__float2half_rn(hf * (1.0f / 4096.0f)));
+}
+
+// FP16-format image of `rows` points: one thread per point and 8-dimension
+// chunk (one 16-byte chunk of each of the six variants).
+__global__ void k1t_pack16_kernel(const float* __restrict__ packed32, int DP, int64_t npts,
+                                  int64_t rows, uint8_t* __restrict__ img) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < rows * 2;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = e >> 1;
+    const int c = (int)(e & 1);
+    uint16_t h[6][8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int k = 8 * c + u;
+      const float v = (r < npts && k < DP) ? packed32[(r >> 1) * (2 * DP) + 2 * k + (r & 1)] : 0.0f;
+      split_f16(v * kLog2e, h[0][u], h[1][u], h[2][u]);
+      split_f16(v, h[3][u], h[4][u], h[5][u]);
+    }
+    const int64_t blk = r / kTB;
+    const uint32_t rr = (uint32_t)(r - blk * kTB);
+    uint8_t* base = img + blk * (int64_t)kTImgBlock + k1t16_offset(rr, 8u * c);
+#pragma unroll
+    for (int vv = 0; vv < 6; ++vv) {
+      uint4 q;
+      q.x = (uint32_t)h[vv][0] | ((uint32_t)h[vv][1] << 16);
+      q.y = (uint32_t)h[vv][2] | ((uint32_t)h[vv][3] << 16);
+      q.z = (uint32_t)h[vv][4] | ((uint32_t)h[vv][5] << 16);
+      q.w = (uint32_t)h[vv][6] | ((uint32_t)h[vv][7] << 16);
+      *reinterpret_cast<uint4*>(base + vv * kTVar16) = q;
+    }
+  }
 }
 
 // Image of `rows` points (a multiple of 512) from the packed FP32 layout
@@ -204,12 +266,13 @@ __device__ __forceinline__ void epi_bar_sync() {
   asm volatile("bar.sync 1, %0;" ::"n"(N) : "memory");
 }
 
-template <int UT, bool CLAMP, bool BATCHED>
+template <int UT, int FMT, bool CLAMP, bool BATCHED>
 __global__ void __launch_bounds__(kTThreads, 1)
     k1t_matvec(const uint8_t* __restrict__ img, int64_t n, const float* __restrict__ x,
                float* __restrict__ colpart, double* __restrict__ rowpart, SymPlan sp, BatchMap bm,
                int* status, const int* gate) {
-  using Cfg = K1tCfg<UT>;
+  using Cfg = K1tCfg<UT, FMT>;
+  constexpr bool F16 = FMT == kK1tF16;
   constexpr int CW = kTCW;
   constexpr int kTBufs = Cfg::kBufs;
   if (gate && *gate == 0) return;
@@ -294,16 +357,16 @@ __global__ void __launch_bounds__(kTThreads, 1)
         const int64_t ab = wk.row_block();
         if (ab != prev_a) {
           if (!wait_or_abort(a_empty, (uint32_t)((a_issued & 1) ^ 1), status, abort)) break;
-          mbar_arrive_expect_tx(a_full, kTHalf);
-          bulk_g2s(sm + Cfg::kOffA, img + ab * (int64_t)kTImgBlock, kTHalf, a_full);
+          mbar_arrive_expect_tx(a_full, Cfg::kHalf);
+          bulk_g2s(sm + Cfg::kOffA, img + ab * (int64_t)kTImgBlock, Cfg::kHalf, a_full);
           ++a_issued;
           prev_a = ab;
         }
         const int bs = (int)(b_issued & 1);
         if (!wait_or_abort(&b_empty[bs], (uint32_t)(((b_issued >> 1) & 1) ^ 1), status, abort)) break;
-        mbar_arrive_expect_tx(&b_full[bs], kTHalf);
-        bulk_g2s(sm + Cfg::kOffB + bs * kTHalf, img + wk.col_block() * (int64_t)kTImgBlock + kTHalf,
-                 kTHalf, &b_full[bs]);
+        mbar_arrive_expect_tx(&b_full[bs], Cfg::kHalf);
+        bulk_g2s(sm + Cfg::kOffB + bs * Cfg::kHalf,
+                 img + wk.col_block() * (int64_t)kTImgBlock + Cfg::kHalf, Cfg::kHalf, &b_full[bs]);
         ++b_issued;
         more = wk.next<BATCHED>(sp, bm, n);
       }
@@ -311,17 +374,20 @@ __global__ void __launch_bounds__(kTThreads, 1)
   } else if (warp == kTMmaWarp) {
     // ---- MMA issue --------------------------------------------------------------
     if (lane == 0) {
-      const uint32_t idesc = tf32_idesc_mn(128, kTSlabN);
+      const uint32_t idesc = F16 ? f16_idesc_mn(128, kTSlabN) : tf32_idesc_mn(128, kTSlabN);
       // descriptors built once: the start-address field holds address >> 4,
       // so an operand offset is added to the descriptor as offset >> 4 (no
       // carry: shared addresses stay below 256 KB)
-      const uint64_t a_hi0 = kmajor_desc_raw(smem_u32(sm + Cfg::kOffA), kTSBO, kTLayout);
-      const uint64_t b_hi0 = kmajor_desc_raw(smem_u32(sm + Cfg::kOffB), kTSBO, kTLayout);
-      constexpr uint64_t kRowTileStep = (128u * kTRowBytes) >> 4;  // next row tile
-      constexpr uint64_t kSlabStep = (kTSlabN * kTRowBytes) >> 4;  // next column slab
-      constexpr uint64_t kLoStep = kTVar >> 4;                     // hi -> lo variant
-      constexpr uint64_t kStageStep = kTHalf >> 4;                 // next column stage
-      constexpr uint64_t kKStep = 32u >> 4;                        // second 8-wide K step
+      constexpr uint32_t kRB = F16 ? kTRowBytes16 : kTRowBytes;
+      const uint64_t a_hi0 = kmajor_desc_raw(smem_u32(sm + Cfg::kOffA), F16 ? kTSBO16 : kTSBO,
+                                             F16 ? kTLayout16 : kTLayout);
+      const uint64_t b_hi0 = kmajor_desc_raw(smem_u32(sm + Cfg::kOffB), F16 ? kTSBO16 : kTSBO,
+                                             F16 ? kTLayout16 : kTLayout);
+      constexpr uint64_t kRowTileStep = (128u * kRB) >> 4;           // next row tile
+      constexpr uint64_t kSlabStep = (kTSlabN * kRB) >> 4;           // next column slab
+      constexpr uint64_t kLoStep = (F16 ? kTVar16 : kTVar) >> 4;     // next variant
+      constexpr uint64_t kStageStep = Cfg::kHalf >> 4;               // next column stage
+      constexpr uint64_t kKStep = 32u >> 4;                          // TF32: second 8-wide K step
       PairWalk wk = w0;
       int64_t prev_a = -1, na = 0, pc = 0, g = 0;
       bool more = true;
@@ -354,12 +420,19 @@ __global__ void __launch_bounds__(kTThreads, 1)
             const int rt = UT * hp + r2;
             const uint32_t d = tmem_base + (uint32_t)(buf * (UT * kTSlabN) + r2 * kTSlabN);
             const uint64_t ahi = a_hi0 + (uint64_t)rt * kRowTileStep, alo = ahi + kLoStep;
-            mma_tf32(d, ahi, bhi, idesc, 0u);
-            mma_tf32(d, ahi, blo, idesc, 1u);
-            mma_tf32(d, alo, bhi, idesc, 1u);
-            mma_tf32(d, ahi + kKStep, bhi + kKStep, idesc, 1u);
-            mma_tf32(d, ahi + kKStep, blo + kKStep, idesc, 1u);
-            mma_tf32(d, alo + kKStep, bhi + kKStep, idesc, 1u);
+            if constexpr (F16) {
+              // variants H, L, Hs: H H' + Hs L' + L Hs'
+              mma_f16(d, ahi, bhi, idesc, 0u);
+              mma_f16(d, ahi + 2 * kLoStep, blo, idesc, 1u);
+              mma_f16(d, alo, bhi + 2 * kLoStep, idesc, 1u);
+            } else {
+              mma_tf32(d, ahi, bhi, idesc, 0u);
+              mma_tf32(d, ahi, blo, idesc, 1u);
+              mma_tf32(d, alo, bhi, idesc, 1u);
+              mma_tf32(d, ahi + kKStep, bhi + kKStep, idesc, 1u);
+              mma_tf32(d, ahi + kKStep, blo + kKStep, idesc, 1u);
+              mma_tf32(d, alo + kKStep, bhi + kKStep, idesc, 1u);
+            }
           }
           mma_any = true;
           mma_commit(&acc_full[buf]);
@@ -523,20 +596,20 @@ __global__ void __launch_bounds__(kTThreads, 1)
   }
 }
 
-template <int UT, bool CLAMP, bool BATCHED>
+template <int UT, int FMT, bool CLAMP, bool BATCHED>
 cudaError_t launch_k1t_t(const uint8_t* img, int64_t n, const float* x, double* rowpart,
                          float* colpart, const SymPlan& sp, const BatchMap& bm, int* status,
                          const int* gate, cudaStream_t s) {
-  using Cfg = K1tCfg<UT>;
+  using Cfg = K1tCfg<UT, FMT>;
   static bool attr = false;
   if (!attr) {
-    const cudaError_t e = cudaFuncSetAttribute(k1t_matvec<UT, CLAMP, BATCHED>,
+    const cudaError_t e = cudaFuncSetAttribute(k1t_matvec<UT, FMT, CLAMP, BATCHED>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)Cfg::kSmemBytes);
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  k1t_matvec<UT, CLAMP, BATCHED><<<sp.grid, kTThreads, Cfg::kSmemBytes, s>>>(
+  k1t_matvec<UT, FMT, CLAMP, BATCHED><<<sp.grid, kTThreads, Cfg::kSmemBytes, s>>>(
       img, n, x, colpart, rowpart, sp, bm, status, gate);
   return cudaGetLastError();
 }
@@ -548,10 +621,16 @@ int k1t_unit_tiles() { return variant_get(LAKER_VARIANT_K1T_UNIT); }
 template <bool CLAMP, bool BATCHED>
 cudaError_t launch_k1t_ut(const uint8_t* img, int64_t n, const float* x, double* rowpart,
                           float* colpart, const SymPlan& sp, const BatchMap& bm, int* status,
-                          const int* gate, cudaStream_t s) {
+                          const int* gate, cudaStream_t s, int fmt) {
+  if (fmt == kK1tF16) {
+    // FP16 operands only for unclamped operators (|e_k| < 9: no overflow)
+    if (CLAMP) return cudaErrorInvalidValue;
+    return launch_k1t_t<4, kK1tF16, false, BATCHED>(img, n, x, rowpart, colpart, sp, bm, status,
+                                                     gate, s);
+  }
   return k1t_unit_tiles() == 2
-             ? launch_k1t_t<2, CLAMP, BATCHED>(img, n, x, rowpart, colpart, sp, bm, status, gate, s)
-             : launch_k1t_t<4, CLAMP, BATCHED>(img, n, x, rowpart, colpart, sp, bm, status, gate, s);
+             ? launch_k1t_t<2, kK1tTf32, CLAMP, BATCHED>(img, n, x, rowpart, colpart, sp, bm, status, gate, s)
+             : launch_k1t_t<4, kK1tTf32, CLAMP, BATCHED>(img, n, x, rowpart, colpart, sp, bm, status, gate, s);
 }
 
 }  // namespace
@@ -563,6 +642,10 @@ bool k1t_enabled(int d) {
     v = (e && e[0] == '0') ? 0 : 1;
   }
   return v == 1 && d >= 1 && d <= 16;
+}
+
+int k1t_format(int clamp) {
+  return (!clamp && variant_get(LAKER_VARIANT_K1T_LOGITS) == 1) ? kK1tF16 : kK1tTf32;
 }
 
 size_t k1t_image_bytes(int64_t points) {
@@ -589,28 +672,33 @@ SymPlan k1t_plan(int64_t n) {
 }
 
 cudaError_t launch_k1t_pack(const float* packed32, int64_t npts, int d, uint8_t* img, int64_t rows,
-                            cudaStream_t s) {
-  if (rows % kTB != 0 || d < 1 || d > 16) return cudaErrorInvalidValue;
-  int g = (int)ceil_div(rows * 4, 256);
+                            cudaStream_t s, int fmt) {
+  if (rows % kTB != 0 || d < 1 || d > 16 || (fmt != kK1tTf32 && fmt != kK1tF16))
+    return cudaErrorInvalidValue;
+  const int per_point = fmt == kK1tF16 ? 2 : 4;  // threads per point
+  int g = (int)ceil_div(rows * per_point, 256);
   if (g > sm_count() * 8) g = sm_count() * 8;
   if (g < 1) g = 1;
-  k1t_pack_kernel<<<g, 256, 0, s>>>(packed32, padded_dim(d), npts, rows, img);
+  if (fmt == kK1tF16)
+    k1t_pack16_kernel<<<g, 256, 0, s>>>(packed32, padded_dim(d), npts, rows, img);
+  else
+    k1t_pack_kernel<<<g, 256, 0, s>>>(packed32, padded_dim(d), npts, rows, img);
   return cudaGetLastError();
 }
 
 cudaError_t launch_k1t(const uint8_t* img, int64_t n, int clamp, const float* x, double* rowpart,
                        float* colpart, const SymPlan& sp, int* status, const int* gate,
-                       cudaStream_t s) {
+                       cudaStream_t s, int fmt) {
   const BatchMap none{};
-  return clamp ? launch_k1t_ut<true, false>(img, n, x, rowpart, colpart, sp, none, status, gate, s)
-               : launch_k1t_ut<false, false>(img, n, x, rowpart, colpart, sp, none, status, gate, s);
+  return clamp ? launch_k1t_ut<true, false>(img, n, x, rowpart, colpart, sp, none, status, gate, s, fmt)
+               : launch_k1t_ut<false, false>(img, n, x, rowpart, colpart, sp, none, status, gate, s, fmt);
 }
 
 cudaError_t launch_k1t_batched(const uint8_t* img, int clamp, const float* x, double* rowpart,
                                float* colpart, const SymPlan& sp, const BatchMap& bm, int* status,
-                               const int* gate, cudaStream_t s) {
-  return clamp ? launch_k1t_ut<true, true>(img, 0, x, rowpart, colpart, sp, bm, status, gate, s)
-               : launch_k1t_ut<false, true>(img, 0, x, rowpart, colpart, sp, bm, status, gate, s);
+                               const int* gate, cudaStream_t s, int fmt) {
+  return clamp ? launch_k1t_ut<true, true>(img, 0, x, rowpart, colpart, sp, bm, status, gate, s, fmt)
+               : launch_k1t_ut<false, true>(img, 0, x, rowpart, colpart, sp, bm, status, gate, s, fmt);
 }
 
 }  // namespace laker

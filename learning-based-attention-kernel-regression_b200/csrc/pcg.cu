@@ -446,7 +446,8 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
   h.active = 1;
   cudaError_t e = cudaMemsetAsync(w.hdr, 0, kWsHeader, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(w.st, &h, sizeof(PcgState), cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess && tc) e = launch_k1t_pack(op->packed32, n, d, w.img, sp.nb * sp.B, s);
+  const int tfmt = k1t_format(op->clamp);  // image format: the pack and every launch
+  if (e == cudaSuccess && tc) e = launch_k1t_pack(op->packed32, n, d, w.img, sp.nb * sp.B, s, tfmt);
   if (e != cudaSuccess) return fail_cuda(e);
 
   int launches = tc ? 1 : 0;
@@ -506,7 +507,7 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
   auto iteration = [&](cudaStream_t cs, bool timed) {
     if (timed) t32.begin(cs);
     if (tc) {
-      launch_k1t(w.img, n, op->clamp, w.p, sym_row, sym_col, sp, dstatus, &w.st->active, cs);
+      launch_k1t(w.img, n, op->clamp, w.p, sym_row, sym_col, sp, dstatus, &w.st->active, cs, tfmt);
     } else if (sym) {
       launch_k1s(op->packed32, n, d, op->clamp, w.p, sym_row, sym_col, sp, dstatus, &w.st->active, cs);
     } else {

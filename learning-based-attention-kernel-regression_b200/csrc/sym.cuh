@@ -133,19 +133,27 @@ cudaError_t launch_k1s_batched(const float* E32, int d, int clamp, const float* 
 // operand image of k1t_image_bytes(points) bytes (128 KB per 512 points,
 // indexed by point: an instance at seg uses blocks seg / 512 ...).
 bool k1t_enabled(int d);
+// Operand formats of the image: split TF32 (kind::tf32 MMAs, two K steps of
+// 8, three products each) or split FP16 (kind::f16, one K step of 16, three
+// products: H H' + Hs L' + L Hs' with H = fp16(v), L = fp16((v - H) 2^12),
+// Hs = fp16(H 2^-12)), used only for unclamped operators (every |e_k| < 9, so
+// no FP16 overflow).  k1t_format(clamp) is the format a pack and the launches
+// that read its image use (LAKER_VARIANT_K1T_LOGITS).
+constexpr int kK1tTf32 = 0, kK1tF16 = 1;
+int k1t_format(int clamp);
 size_t k1t_image_bytes(int64_t points);
 SymPlan k1t_plan(int64_t n);
 SymPlan k1t_plan_pairs(int64_t nb, int64_t npairs);
 // image of `rows` points (a multiple of 512) from the packed FP32 layout;
 // points at or past npts are zero
 cudaError_t launch_k1t_pack(const float* packed32, int64_t npts, int d, uint8_t* img, int64_t rows,
-                            cudaStream_t s);
+                            cudaStream_t s, int fmt = kK1tTf32);
 cudaError_t launch_k1t(const uint8_t* img, int64_t n, int clamp, const float* x, double* rowpart,
                        float* colpart, const SymPlan& sp, int* status, const int* gate,
-                       cudaStream_t s);
+                       cudaStream_t s, int fmt = kK1tTf32);
 cudaError_t launch_k1t_batched(const uint8_t* img, int clamp, const float* x, double* rowpart,
                                float* colpart, const SymPlan& sp, const BatchMap& bm, int* status,
-                               const int* gate, cudaStream_t s);
+                               const int* gate, cudaStream_t s, int fmt = kK1tTf32);
 // y = lam x + (sum of the partials) for the standalone matvec.
 cudaError_t launch_sym_finish(const SymPlan& sp, const double* rowpart, const float* colpart,
                               int64_t n, float lam, const float* x, float* y, int64_t ldy,

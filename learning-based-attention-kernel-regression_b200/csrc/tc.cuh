@@ -10,8 +10,9 @@ namespace laker {
 
 // Shared-memory matrix descriptor of a K-major operand in a swizzled
 // canonical layout: 8-row core groups `sbo` bytes apart, layout code 2
-// (128-byte swizzle) or 4 (64-byte swizzle), tiles aligned to the swizzle
-// atom.  A K step inside the swizzled row advances the start address.
+// (128-byte swizzle), 4 (64-byte swizzle) or 6 (32-byte swizzle), tiles
+// aligned to the swizzle atom.  A K step inside the swizzled row advances the
+// start address.
 __device__ __forceinline__ uint64_t kmajor_desc_raw(uint32_t saddr, uint32_t sbo, uint32_t layout) {
   uint64_t d = 0;
   d |= (uint64_t)((saddr >> 4) & 0x3FFFu);  // start address [0,14)
@@ -29,6 +30,26 @@ __host__ __device__ constexpr uint32_t tf32_idesc_mn(int m, int n) {
          | (2u << 10)                   // B format TF32
          | ((uint32_t)(n >> 3) << 17)   // N >> 3
          | ((uint32_t)(m >> 4) << 24);  // M >> 4
+}
+
+// Instruction descriptor: kind::f16, D = FP32, A and B both FP16 (format 0),
+// K-major.
+__host__ __device__ constexpr uint32_t f16_idesc_mn(int m, int n) {
+  return (1u << 4)                      // D format F32
+         | (0u << 7)                    // A format F16
+         | (0u << 10)                   // B format F16
+         | ((uint32_t)(n >> 3) << 17)   // N >> 3
+         | ((uint32_t)(m >> 4) << 24);  // M >> 4
+}
+
+__device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                        uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+      :
+      : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
 __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,

@@ -10,8 +10,8 @@
 namespace laker {
 namespace {
 
-constexpr int kNumVariants = 5;
-std::atomic<int> g_variant[kNumVariants] = {{-1}, {-1}, {-1}, {-1}, {-1}};
+constexpr int kNumVariants = 6;
+std::atomic<int> g_variant[kNumVariants] = {{-1}, {-1}, {-1}, {-1}, {-1}, {-1}};
 
 int variant_default(int which) {
   if (which == LAKER_VARIANT_K1T_UNIT) {
@@ -29,6 +29,13 @@ int variant_default(int which) {
     }
     return 6;
   }
+  if (which == LAKER_VARIANT_K1T_LOGITS) {
+    // split FP16 by default: n = 100k, 1.99 vs 2.10 ms per operator launch,
+    // the same accuracy class as split TF32 (4.6e-7 vs 6.7e-7 relative at
+    // n = 20k); LAKER_K1T_F16=0 selects split TF32
+    const char* e = getenv("LAKER_K1T_F16");
+    return (e && e[0] == '0') ? 0 : 1;
+  }
   const char* e = getenv("LAKER_K2_LOGITS_TC");
   return (e && e[0] == '1') ? 1 : 0;
 }
@@ -36,6 +43,7 @@ int variant_default(int which) {
 bool variant_valid(int which, int value) {
   if (which == LAKER_VARIANT_K1T_UNIT) return value == 2 || value == 4;
   if (which == LAKER_VARIANT_SYM_MIN_BLOCKS) return value >= 0 && value <= 64;
+  if (which == LAKER_VARIANT_K1T_LOGITS) return value == 0 || value == 1;
   return value == 0 || value == 1;
 }
 

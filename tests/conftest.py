@@ -45,3 +45,16 @@ def cuda():
     from laker_b200 import _lib
     _lib.load()
     return torch.device("cuda", 0)
+
+
+@pytest.fixture(params=["tf32", "f16"])
+def k1t_logits(request):
+    """The tensor-core symmetric kernel with split-TF32 and split-FP16 logits
+    (LAKER_VARIANT_K1T_LOGITS; an engine keeps the format of its creation)."""
+    from laker_b200 import _lib
+
+    prev = _lib.set_variant(_lib.VARIANT_K1T_LOGITS, 1 if request.param == "f16" else 0)
+    try:
+        yield request.param
+    finally:
+        _lib.set_variant(_lib.VARIANT_K1T_LOGITS, prev)

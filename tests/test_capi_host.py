@@ -84,6 +84,11 @@ def test_variant_switches_without_gpu():
         assert lib.laker_fp32_operator_kernel(2000, 10) != 0  # forced symmetric
         assert lib.laker_fp32_operator_kernel(0, 10) == 0
     assert lib.laker_set_variant(_lib.VARIANT_SYM_MIN_BLOCKS, mb) == 0
+    lg = lib.laker_get_variant(_lib.VARIANT_K1T_LOGITS)
+    assert lg in (0, 1)
+    assert lib.laker_set_variant(_lib.VARIANT_K1T_LOGITS, 2) == -1
+    assert lib.laker_set_variant(_lib.VARIANT_K1T_LOGITS, 1 - lg) == lg
+    assert lib.laker_set_variant(_lib.VARIANT_K1T_LOGITS, lg) == 1 - lg
     assert lib.laker_get_variant(9) == -1 and lib.laker_set_variant(9, 0) == -1
 
 

@@ -41,7 +41,7 @@ def solo(cuda, op, pre, b, tol=1e-7):
     return out[slot]
 
 
-def test_engine_solves_and_matches_solo(cuda):
+def test_engine_solves_and_matches_solo(cuda, k1t_logits):
     from laker_b200 import SolveEngine
 
     probs = [make_problem(cuda, n, s) for s, n in enumerate([300, 1100, 77, 2049])]

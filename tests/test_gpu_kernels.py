@@ -42,20 +42,24 @@ def test_matvec_golden(cuda, golden, key):
         assert rel(op.kernel_eval(q), g[f"{key}_keval"]) < max(tol, 1e-6 if dtype == torch.float32 else 0)
 
 
-@pytest.fixture(params=["default", "symmetric"])
+@pytest.fixture(params=["default", "symmetric", "symmetric-f16"])
 def sym_route(request):
-    """Run once with the default routing (small square operators on the plain
-    kernel) and once with the symmetric kernels forced down to one block."""
+    """Run with the default routing (small square operators on the plain
+    kernel), with the symmetric kernels forced down to one block, and the
+    same with the tensor-core kernel's split-FP16 logits."""
     from laker_b200 import _lib
 
     if request.param == "default":
         yield request.param
         return
     prev = _lib.set_variant(_lib.VARIANT_SYM_MIN_BLOCKS, 0)
+    prev_f = _lib.set_variant(_lib.VARIANT_K1T_LOGITS, 1 if request.param.endswith("f16") else 0)
     try:
         yield request.param
     finally:
         _lib.set_variant(_lib.VARIANT_SYM_MIN_BLOCKS, prev)
+        _lib.set_variant(_lib.VARIANT_K1T_LOGITS, prev_f)
+
 
 
 @pytest.mark.parametrize("n", [1, 2, 3, 255, 256, 257, 511, 513, 1029, 4097])
@@ -76,7 +80,7 @@ def test_matvec_ragged_sizes(cuda, n, sym_route):
 
 
 @pytest.mark.parametrize("n", [20000, 36100])
-def test_symmetric_operator_many_pairs_per_cta(cuda, n):
+def test_symmetric_operator_many_pairs_per_cta(cuda, n, k1t_logits):
     """The operator at sizes where every CTA of the persistent symmetric kernel
     walks several block pairs (row-block changes, operand-stage reuse,
     accumulator-buffer wrap-around; n = 20000: 820 pairs, 36100: 2485 pairs
@@ -93,13 +97,17 @@ def test_symmetric_operator_many_pairs_per_cta(cuda, n):
     y2 = op32.matvec(xd)
     assert torch.equal(y1, y2)
     assert rel(y1, ref) < F32_RTOL
-    # per-row agreement, not only in norm
+    # per-row agreement, not only in norm: entries carry ~1e-6 relative error,
+    # which a row whose sum cancels down to 1e-3 of the largest row amplifies
+    # by up to ~|K||x| / |y_i|; measured worst rows 8e-5 (split TF32) and
+    # 1.6e-4 (split FP16) at n = 20000, 7e-5 and 1.7e-5 at n = 36100
     err = np.abs(y1.cpu().double().numpy() - ref) / np.maximum(np.abs(ref), 1e-3 * np.abs(ref).max())
-    assert err.max() < 1e-4
+    assert err.max() < 3e-4
+    assert np.quantile(err, 0.999) < 1e-4
 
 
 @pytest.mark.parametrize("d", [1, 2, 3, 5, 8, 11, 16])
-def test_matvec_all_dims(cuda, d):
+def test_matvec_all_dims(cuda, d, sym_route):
     from laker_b200 import AttentionKernelOperator
 
     rng = np.random.default_rng(100 + d)
