@@ -432,9 +432,12 @@ def roofline_block(kernel_id, work, k1_avg_ms, achieved, exps_per_s, peaks, traf
 
     Tensor-core logits (kernel 2): per entry evaluated the CUDA cores do one
     MUFU exp2 and two FMAs (one for an entry on a diagonal block pair), so the
-    binding unit is the exp2 rate; the logits add 3 split-TF32 products x 2 x
-    16 flops per entry on the tensor cores.  CUDA-core logits (kernel 1):
-    d + 2 FMAs per entry, bound by the FFMA rate."""
+    binding unit is the exp2 rate; the logits add 3 split products x 2 x 16
+    flops per entry on the tensor cores (split FP16 by default, kind::f16,
+    against the dense FP16 rate = the bf16 figure; split TF32 against half of
+    it).  CUDA-core logits (kernel 1): d + 2 FMAs per entry, bound by the FFMA
+    rate."""
+    from laker_b200 import _lib
     common = {
         "traffic": traffic,
         "avg_launch_ms": k1_avg_ms,
@@ -444,11 +447,16 @@ def roofline_block(kernel_id, work, k1_avg_ms, achieved, exps_per_s, peaks, traf
     }
     if kernel_id == 2:
         peak = peaks["mufu_tops"] * 1e12
+        f16 = _lib.get_variant(_lib.VARIANT_K1T_LOGITS) == 1
         tf32 = work["entries"] * 96.0 / (k1_avg_ms * 1e-3) / 1e12
         tf32_peak, tf32_src = _tf32_peak()
+        if f16:
+            tf32_peak, tf32_src = 2.0 * tf32_peak, tf32_src.replace("half the", "the").replace(
+                "TF32 dense rate", "FP16 dense rate")
         return dict(common, **{
             "bound": "mufu",
-            "kernel": "k1t_matvec (symmetric FP32 operator, split-TF32 tcgen05 logits)",
+            "kernel": "k1t_matvec (symmetric FP32 operator, split-%s tcgen05 logits)"
+                      % ("FP16" if f16 else "TF32"),
             "achieved": exps_per_s / 1e12, "peak": peaks["mufu_tops"], "unit": "Texp2/s",
             "frac": exps_per_s / peak,
             "peak_source": "MUFU ex2 microbenchmark measured in this run (laker_measure_peaks)",

@@ -114,10 +114,10 @@ int laker_fp32_matvec_work(int64_t n, int d, double* entries, double* flops, dou
  * LAKER_VARIANT_SYM_MIN_BLOCKS x 512 points, default 3072, where the
  * symmetric kernels have too few block pairs to fill the GPU), 1 the
  * symmetric kernel with logits on the CUDA cores, 2 the symmetric kernel with
- * logits on the tensor cores (split-TF32 tcgen05 MMAs; then `flops` above
- * counts only the CUDA-core accumulation FMAs and the logits add 3 x 2 x 16
- * TF32 tensor flops per entry evaluated); -1 for invalid arguments.  No
- * counterpart in the reference. */
+ * logits on the tensor cores (split-FP16 or split-TF32 tcgen05 MMAs,
+ * LAKER_VARIANT_K1T_LOGITS; then `flops` above counts only the CUDA-core
+ * accumulation FMAs and the logits add 3 x 2 x 16 tensor flops per entry
+ * evaluated); -1 for invalid arguments.  No counterpart in the reference. */
 int laker_fp32_operator_kernel(int64_t n, int d);
 
 /* Kernel variant choices, changeable between calls (no call may be in flight
