@@ -2,8 +2,9 @@
 
 The fused kernels have a few tile and pipeline choices whose best value
 depends on the problem size and the GPU (include/laker_b200.h,
-LAKER_VARIANT_*): the TMEM unit of the tensor-core symmetric operator (4 or 2
-row tiles per accumulator buffer) and, per class of multi-RHS chunk width
+LAKER_VARIANT_*): the logit operands of the tensor-core symmetric operator
+(split FP16 or split TF32), its TMEM unit with split TF32 (4 or 2 row tiles
+per accumulator buffer) and, per class of multi-RHS chunk width
 (<= 32, 33..128, > 128 right-hand sides), whether the multi-RHS kernel takes
 its logits from the tensor cores or the CUDA cores.  `autotune` times every
 candidate with CUDA events on a synthetic problem of the caller's size (the
@@ -23,7 +24,7 @@ from . import _lib
 from .kernels import AttentionKernelOperator
 
 # agreement required between two variants of the same product (relative,
-# per output column): the split-TF32 products differ at ~1e-6
+# per output column): the split-TF32 / split-FP16 products differ at ~1e-6
 AGREE_RTOL = 1e-4
 
 
@@ -97,7 +98,10 @@ def autotune(n: int = 20000, d: int = 10, ks: Sequence[int] = (16, 64, 256), rep
 
     if _lib.fp32_operator_kernel(n, d) == 2:
         x = torch.randn(n, generator=g).to(dev, torch.float32)
-        pick("k1t_unit", _lib.VARIANT_K1T_UNIT, (4, 2), lambda: op.matvec(x))
+        if op.skip_clamp:  # clamped operators always take split TF32
+            pick("k1t_logits", _lib.VARIANT_K1T_LOGITS, (1, 0), lambda: op.matvec(x))
+        if _lib.get_variant(_lib.VARIANT_K1T_LOGITS) == 0 or not op.skip_clamp:
+            pick("k1t_unit", _lib.VARIANT_K1T_UNIT, (4, 2), lambda: op.matvec(x))
     by_slot: Dict[int, int] = {}
     for k in ks:
         if k > 1:

@@ -15,10 +15,13 @@ def test_autotune_picks_variants_and_keeps_results(cuda):
     import laker_b200 as L
     from laker_b200 import _lib
 
-    before = {w: _lib.get_variant(w) for w in range(4)}
+    before = {w: _lib.get_variant(w) for w in range(6)}
     try:
-        res = L.autotune(n=3000, d=10, ks=(16, 100, 256), reps=2, device=cuda)
-        assert set(res) >= {"k2_logits_n32", "k2_logits_n128", "k2_logits_wide"}
+        # n = 4000: above the plain-kernel threshold, so the tensor-core
+        # symmetric operator's variants are timed too
+        res = L.autotune(n=4000, d=10, ks=(16, 100, 256), reps=2, device=cuda)
+        assert set(res) >= {"k1t_logits", "k2_logits_n32", "k2_logits_n128", "k2_logits_wide"}
+        assert _lib.get_variant(_lib.VARIANT_K1T_LOGITS) == res["k1t_logits"]["choice"]
         for name, r in res.items():
             assert r["choice"] in r["ms"] and all(t > 0 for t in r["ms"].values())
         assert _lib.get_variant(_lib.VARIANT_K2_LOGITS_WIDE) == res["k2_logits_wide"]["choice"]
