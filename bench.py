@@ -932,6 +932,43 @@ def workload_batch(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def serve_cpu_estimate(trace, recs, n_sample: int = 8) -> dict:
+    """CPU baseline of a served trace: the float64 oracle's operator cost for
+    an evenly spaced sample of the requests, extrapolated.  Per request: the
+    operator on 256 of its n rows (all k right-hand sides: 1 for a fit, m for a
+    variance query), scaled to n rows, times the PCG iterations the GPU solve
+    of that request took, plus for a fit the CCCP build's operator on its N_r
+    probes.  Timing depends only on the shapes, so seeded random embeddings
+    of the request's size stand in."""
+    from oracle import laker_oracle as O
+
+    rng = np.random.default_rng(0)
+    by_rid = {r.rid: r for r in trace}
+    sample = trace[:: max(1, len(trace) // n_sample)][:n_sample]
+    total = 0.0
+
+    def timed_rows(E, X, rows):
+        t0 = time.perf_counter()
+        O.rect_matvec(E[:rows], E, X)
+        return (time.perf_counter() - t0) * E.shape[0] / rows
+
+    for r in sample:
+        n = r.n if r.kind == "fit" else by_rid[r.target].n
+        k = 1 if r.kind == "fit" else r.m
+        rows = min(n, 256)
+        E = rng.standard_normal((n, EMBED_DIM)) * 0.3
+        X = rng.standard_normal(n) if k == 1 else rng.standard_normal((n, k))
+        total += max(1, recs[r.rid].iterations) * timed_rows(E, X, rows)
+        if r.kind == "fit":
+            nr = min(n, max(200, int(2 * n ** 0.5)))
+            total += timed_rows(E, rng.standard_normal((n, nr)), rows)
+    return {"value": len(sample) / total, "unit": "requests/s", "cores": O.c_threads(),
+            "kind": "port",
+            "sample": f"float64 oracle operator for {len(sample)} of {len(trace)} requests "
+                      f"(256 rows per request scaled to n, x the request's PCG iterations, + the "
+                      f"CCCP probe product of fits): {total:.1f} s extrapolated"}
+
+
 def workload_serve(args) -> None:
     """Config: Poisson trace of fit (70 %) and variance (30 %) requests."""
     import laker_b200  # noqa: F401
@@ -949,6 +986,7 @@ def workload_serve(args) -> None:
         clocks.start()
         recs = srv.run(trace)
         clocks.stop()
+        last_trace, last_recs = trace, recs
         s = summarize(recs)
         s["activity_s"] = dict(srv.stats)
         s["clocks"] = clocks.summary()
@@ -969,6 +1007,8 @@ def workload_serve(args) -> None:
                        "rates": rates})
     line.update({"p50_ms": best["served"]["p50_ms"], "p99_ms": best["served"]["p99_ms"],
                  "clocks": best["served"]["clocks"], "by_rate": out})
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = serve_cpu_estimate(last_trace, last_recs)
     print(json.dumps(line), flush=True)
 
 
