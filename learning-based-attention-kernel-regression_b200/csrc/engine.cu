@@ -153,25 +153,45 @@ __device__ void project_block(const EngineDev& ed, const BlockCtx& c, const doub
   }
 }
 
-// Last block of an instance: u = sum of the block projections (block order),
-// v = W u -> vvec[k].  s_u may alias the projection scratch (the arrival
-// barrier separates the two uses).
+// Last block of an instance: u = sum of the block projections, v = W u ->
+// vvec[k].  Both sums run as four interleaved partial sums (index mod 4)
+// combined in a fixed order, so that four loads are in flight per thread
+// instead of one dependent chain; the result depends only on the instance.
+// s_u may alias the projection scratch (the arrival barrier separates the two
+// uses).
 __device__ void w_multiply(const EngineDev& ed, const BlockCtx& c, double* s_u) {
   const SlotInfo& si = ed.slots[c.k];
   const int nr = si.nr, ldq = si.ldq;
   const float* W = reinterpret_cast<const float*>(si.w);
   for (int col = threadIdx.x; col < nr; col += BT) {
-    double u = 0.0;
-    for (unsigned b = 0; b < c.nblk; ++b) u += (double)__ldcg(ed.upart + (c.b0 + b) * ed.ustride + col);
-    s_u[col] = u;
+    const float* up = ed.upart + c.b0 * ed.ustride + col;
+    double u0 = 0.0, u1 = 0.0, u2 = 0.0, u3 = 0.0;
+    unsigned b = 0;
+    for (; b + 4 <= c.nblk; b += 4) {
+      u0 += (double)__ldcg(up + (int64_t)b * ed.ustride);
+      u1 += (double)__ldcg(up + (int64_t)(b + 1) * ed.ustride);
+      u2 += (double)__ldcg(up + (int64_t)(b + 2) * ed.ustride);
+      u3 += (double)__ldcg(up + (int64_t)(b + 3) * ed.ustride);
+    }
+    for (; b < c.nblk; ++b) u0 += (double)__ldcg(up + (int64_t)b * ed.ustride);
+    s_u[col] = (u0 + u1) + (u2 + u3);
   }
   __syncthreads();
   float* v = ed.vvec + (int64_t)c.k * ed.ustride;
   for (int col = threadIdx.x; col < ldq; col += BT) {
-    double a = 0.0;
-    if (col < nr)
-      for (int cc = 0; cc < nr; ++cc) a = fma((double)W[(int64_t)cc * nr + col], s_u[cc], a);
-    v[col] = (float)a;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    if (col < nr) {
+      const float* wc = W + col;
+      int cc = 0;
+      for (; cc + 4 <= nr; cc += 4) {
+        a0 = fma((double)wc[(int64_t)cc * nr], s_u[cc], a0);
+        a1 = fma((double)wc[(int64_t)(cc + 1) * nr], s_u[cc + 1], a1);
+        a2 = fma((double)wc[(int64_t)(cc + 2) * nr], s_u[cc + 2], a2);
+        a3 = fma((double)wc[(int64_t)(cc + 3) * nr], s_u[cc + 3], a3);
+      }
+      for (; cc < nr; ++cc) a0 = fma((double)wc[(int64_t)cc * nr], s_u[cc], a0);
+    }
+    v[col] = (float)((a0 + a1) + (a2 + a3));
   }
 }
 
