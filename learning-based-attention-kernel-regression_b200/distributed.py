@@ -174,9 +174,8 @@ class ShardedPreconditioner:
 
     @classmethod
     def from_cccp(cls, pc: CCCPPreconditioner, r0: int, r1: int) -> "ShardedPreconditioner":
-        if pc.q_basis is None or pc._w32 is None:
-            raise RuntimeError("Preconditioner has not been built. Call build() first.")
-        return cls(pc.q_basis[r0:r1], pc._w32, pc.isotropic_coef ** (-0.5))
+        _, w32, _, cis = pc.apply_factors()  # raises before the first build
+        return cls(pc.q_basis[r0:r1], w32, cis)
 
 
 def _precondition(r: torch.Tensor, pre: Optional[ShardedPreconditioner], exch: RowExchange):

@@ -334,6 +334,13 @@ class CCCPPreconditioner:
         pre._c = _lib.precond_struct(pre._q32, pre._w32, pre.n, pre.nr, pre.isotropic_coef ** (-0.5))
         return pre
 
+    def apply_factors(self):
+        """(Q padded to a multiple of 4 columns in FP32, the folded W in FP32,
+        N_r, c^-1/2): the factors the fused apply uses, P = c^-1/2 I + Q W Q^T."""
+        if self._c is None:
+            raise RuntimeError("Preconditioner has not been built. Call build() first.")
+        return self._q32, self._w32, self.nr, self.isotropic_coef ** (-0.5)
+
     def c_precond(self) -> _lib.laker_precond:
         if self._c is None:
             raise RuntimeError("Preconditioner has not been built. Call build() first.")
@@ -352,9 +359,8 @@ class CCCPPreconditioner:
 
     def apply_1d(self, x: torch.Tensor) -> torch.Tensor:
         _lib.require_cuda(x, "x")
-        self.c_precond()  # raises before the first build
-        return ops.precond_apply(self._q32, self._w32, self.n, self.nr,
-                                 self.isotropic_coef ** (-0.5), x, x.dtype == torch.float64)
+        q32, w32, nr, cis = self.apply_factors()
+        return ops.precond_apply(q32, w32, self.n, nr, cis, x, x.dtype == torch.float64)
 
     def apply_2d(self, x: torch.Tensor) -> torch.Tensor:
         _lib.require_cuda(x, "x")

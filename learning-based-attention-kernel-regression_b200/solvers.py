@@ -138,15 +138,11 @@ class PreconditionedConjugateGradient:
     def _solve_fused(self, op: AttentionKernelOperator, pc: Optional[CCCPPreconditioner],
                      rhs: torch.Tensor, x0: Optional[torch.Tensor], max_iter: int) -> torch.Tensor:
         p = op.packed
-        if pc is not None:
-            pc.c_precond()  # raises before the first build
+        q32, w32, nr, cis = pc.apply_factors() if pc is not None else (None, None, 0, 0.0)
         x, stats = ops.pcg_solve(
             p.packed32, p.packed64, op.n, op.embedding_dim, op.lambda_reg, not op.skip_clamp,
-            pc._q32 if pc is not None else None, pc._w32 if pc is not None else None,
-            pc.nr if pc is not None else 0,
-            pc.isotropic_coef ** (-0.5) if pc is not None else 0.0, rhs, x0, self.tol,
-            int(max_iter), self.reliable_delta, self._eps(rhs.dtype), self.check_every,
-            self.profile)
+            q32, w32, nr, cis, rhs, x0, self.tol, int(max_iter), self.reliable_delta,
+            self._eps(rhs.dtype), self.check_every, self.profile)
         res = ops.result_from_stats(stats)
         self.last_result = res
         self.iterations = int(res.iterations)

@@ -61,11 +61,12 @@ def test_solve_and_precond_ops(cuda):
                             dtype=torch.float32).build(op.matvec, n, seed=2)
     bt = torch.tensor(b, device=cuda)
     cis = pc.isotropic_coef ** -0.5
-    pargs = (pc._q32, pc._w32, n, pc.nr, cis, bt, True)
+    q32, w32, nr, cis = pc.apply_factors()
+    pargs = (q32, w32, n, nr, cis, bt, True)
     torch.library.opcheck(ops.precond_apply.default, pargs, test_utils=CHECKS)
     assert torch.equal(ops.precond_apply(*pargs), pc.apply(bt))
     p = op.packed
-    sargs = (p.packed32, p.packed64, n, 10, lam, False, pc._q32, pc._w32, pc.nr, cis, bt, None,
+    sargs = (p.packed32, p.packed64, n, 10, lam, False, q32, w32, nr, cis, bt, None,
              1e-8, 2000, 0.03, 1e-8, 0, False)
     torch.library.opcheck(ops.pcg_solve.default, sargs, test_utils=CHECKS)
     x, stats = ops.pcg_solve(*sargs)
