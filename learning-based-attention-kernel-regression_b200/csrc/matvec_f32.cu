@@ -233,24 +233,40 @@ int k1_variant(int dp) {
 // 4 x 4 register microtiles.  Row sums are flushed to FP64 every 256 columns.
 // Real = float: exp2 on MUFU with log2 e folded into the rows; Real = double:
 // FP64 logits and exp (the accurate operator, optionally as a residual).
+// Narrow products (k <= 16, e.g. the FP64 residual of a variance solve with
+// few queries) use 64 x 16 tiles of 64 threads instead, so that no
+// accumulation FMA lands on an absent right-hand side (LAKER_MULTI_NARROW=0
+// keeps the 64-wide tile for comparisons).
 // ---------------------------------------------------------------------------
 constexpr int kMBM = 64, kMBN = 64, kMBK = 32, kMThreads = 256;
+constexpr int kMBNNarrow = 16;
+
+bool multi_narrow_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("LAKER_MULTI_NARROW");
+    v = (e && e[0] == '0') ? 0 : 1;
+  }
+  return v == 1;
+}
 
 }  // namespace
 
-template <typename Real, int DP, bool CLAMP, bool RESIDUAL>
-__global__ void __launch_bounds__(kMThreads)
+template <typename Real, int DP, bool CLAMP, bool RESIDUAL, int BN = kMBN>
+__global__ void __launch_bounds__((kMBM / 4) * (BN / 4))
     multi_matvec_kernel(const Real* __restrict__ rows, int64_t m, const Real* __restrict__ cols,
                         int64_t n, int col_layout_pairs, Real lam, const Real* __restrict__ X,
                         int k, int64_t ldx, const Real* __restrict__ B, int64_t ldb,
                         Real* __restrict__ Y, int64_t ldy, int row_layout_pairs) {
+  constexpr int T = (kMBM / 4) * (BN / 4);  // threads: one 4 x 4 microtile each
+  static_assert(T % kMBM == 0 && (kMBM * kMBK) % T == 0, "tile / thread mapping");
   __shared__ __align__(16) Real sCol[kMBK][DP + 1];
   __shared__ __align__(16) Real sP[kMBK][kMBM];
-  __shared__ __align__(16) Real sX[kMBK][kMBN];
+  __shared__ __align__(16) Real sX[kMBK][BN];
   const int tid = threadIdx.x;
-  const int tx = tid & 15, ty = tid >> 4;
+  const int tx = tid % (BN / 4), ty = tid / (BN / 4);
   const int64_t i0 = (int64_t)blockIdx.x * kMBM;
-  const int64_t c0 = (int64_t)blockIdx.y * kMBN;
+  const int64_t c0 = (int64_t)blockIdx.y * BN;
 
   auto emb = [&](const Real* base, int pairs, int64_t i, int kk) -> Real {
     return pairs ? base[(i >> 1) * (DP * 2) + 2 * kk + (i & 1)] : base[i * DP + kk];
@@ -278,20 +294,20 @@ __global__ void __launch_bounds__(kMThreads)
   const int nsteps = (int)ceil_div(n, kMBK);
   for (int st = 0; st < nsteps; ++st) {
     const int64_t j0 = (int64_t)st * kMBK;
-    for (int o = tid; o < kMBK * DP; o += kMThreads) {
+    for (int o = tid; o < kMBK * DP; o += T) {
       const int jj = o / DP, kk = o - jj * DP;
       const int64_t j = j0 + jj;
       sCol[jj][kk] = (j < n) ? emb(cols, col_layout_pairs, j, kk) : Real(0);
     }
-    for (int o = tid; o < kMBK * kMBN; o += kMThreads) {
-      const int jj = o / kMBN, cc = o - jj * kMBN;
+    for (int o = tid; o < kMBK * BN; o += T) {
+      const int jj = o / BN, cc = o - jj * BN;
       const int64_t j = j0 + jj, c = c0 + cc;
       sX[jj][cc] = (j < n && c < k) ? X[j * ldx + c] : Real(0);
     }
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < (kMBM * kMBK) / kMThreads; ++q) {
-      const int jj = (tid >> 6) + 4 * q;
+    for (int q = 0; q < (kMBM * kMBK) / T; ++q) {
+      const int jj = tid / kMBM + (T / kMBM) * q;
       Real s = rv[0] * sCol[jj][0];
 #pragma unroll
       for (int kk = 1; kk < DP; ++kk) s = fma(rv[kk], sCol[jj][kk], s);
@@ -348,6 +364,13 @@ template <int DP, bool CLAMP>
 cudaError_t launch_multi_f32_t(const float* rows, int64_t m, const float* cols, int64_t n, float lam,
                                const float* X, int k, int64_t ldx, float* Y, int64_t ldy,
                                cudaStream_t s) {
+  if (k <= kMBNNarrow && multi_narrow_enabled()) {
+    dim3 grid((unsigned)ceil_div(m, kMBM), 1);
+    multi_matvec_kernel<float, DP, CLAMP, false, kMBNNarrow>
+        <<<grid, (kMBM / 4) * (kMBNNarrow / 4), 0, s>>>(rows, m, cols, n, 1, lam, X, k, ldx, nullptr,
+                                                        0, Y, ldy, 1);
+    return cudaGetLastError();
+  }
   dim3 grid((unsigned)ceil_div(m, kMBM), (unsigned)ceil_div(k, kMBN));
   multi_matvec_kernel<float, DP, CLAMP, false><<<grid, kMThreads, 0, s>>>(
       rows, m, cols, n, 1, lam, X, k, ldx, nullptr, 0, Y, ldy, 1);
@@ -358,6 +381,17 @@ template <int DP, bool CLAMP>
 cudaError_t launch_multi_f64_t(const double* rows, int64_t m, const double* cols, int64_t n,
                                double lam, const double* X, int k, int64_t ldx, const double* B,
                                int64_t ldb, double* Y, int64_t ldy, cudaStream_t s) {
+  if (k <= kMBNNarrow && multi_narrow_enabled()) {
+    dim3 grid((unsigned)ceil_div(m, kMBM), 1);
+    constexpr int T = (kMBM / 4) * (kMBNNarrow / 4);
+    if (B)
+      multi_matvec_kernel<double, DP, CLAMP, true, kMBNNarrow><<<grid, T, 0, s>>>(
+          rows, m, cols, n, 0, lam, X, k, ldx, B, ldb, Y, ldy, 0);
+    else
+      multi_matvec_kernel<double, DP, CLAMP, false, kMBNNarrow><<<grid, T, 0, s>>>(
+          rows, m, cols, n, 0, lam, X, k, ldx, nullptr, 0, Y, ldy, 0);
+    return cudaGetLastError();
+  }
   dim3 grid((unsigned)ceil_div(m, kMBM), (unsigned)ceil_div(k, kMBN));
   if (B)
     multi_matvec_kernel<double, DP, CLAMP, true><<<grid, kMThreads, 0, s>>>(
