@@ -18,8 +18,13 @@
  *     asynchronous on that stream except laker_pcg_solve, which synchronises
  *     the stream to poll convergence and returns when the solve has ended.
  *   - Every entry point returns a laker status code (0 = LAKER_OK).  Kernels
- *     never trap; device-side failures (a bounded wait that expired) are
- *     reported through the status code after the stream synchronises.
+ *     never trap.  A device-side failure (a bounded wait that expired) is
+ *     recorded in the status word at the start of the call's workspace (or of
+ *     the allocation-free entry point's scratch): the asynchronous products
+ *     then write NaN to every output element, laker_workspace_status /
+ *     laker_noalloc_status read the word back after the stream synchronises,
+ *     and the synchronising calls (laker_pcg_solve, the engine) return it as
+ *     their status.
  *
  * Reference interfaces cited as path:line are in the LAKER Python package
  * (laker/kernels.py, laker/solvers.py, laker/preconditioner.py, laker/core.py).
@@ -60,6 +65,14 @@ const char* laker_status_string(int status);
 
 /* cudaError_t of the most recent LAKER_ERR_CUDA on the calling thread. */
 int laker_last_cuda_error(void);
+
+/* Device status word of the last call that used `workspace` (a workspace of
+ * laker_attn_matvec_f32 / _f64): synchronises `stream` and writes LAKER_OK or
+ * the device-side failure (LAKER_ERR_TIMEOUT) to *status.  The outputs of a
+ * failed call are NaN.  No counterpart in the reference, whose products are
+ * synchronous torch calls that raise (laker/solvers.py:343-352 raises on
+ * breakdown). */
+int laker_workspace_status(const void* workspace, int* status, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Embedding layouts                                                         */
@@ -149,6 +162,17 @@ int laker_fp32_operator_kernel(int64_t n, int d);
 #define LAKER_VARIANT_K2_LOGITS_WIDE 3
 #define LAKER_VARIANT_SYM_MIN_BLOCKS 4
 #define LAKER_VARIANT_K1T_LOGITS 5
+/*   LAKER_VARIANT_WAIT_LIMIT_US  time limit of the kernels' bounded pipeline
+ *                                waits in microseconds, 0..2000000 (default
+ *                                2000000).  It applies on the current device
+ *                                (set it once per device).  0 makes every
+ *                                pipeline wait give up at once: the kernels
+ *                                then drain their copies and tensor-core
+ *                                operations in flight (always with the full
+ *                                limit), record LAKER_ERR_TIMEOUT and return,
+ *                                which runs the failure path deterministically
+ *                                without a fault or a hang. */
+#define LAKER_VARIANT_WAIT_LIMIT_US 6
 int laker_set_variant(int which, int value);
 int laker_get_variant(int which);
 
@@ -171,6 +195,13 @@ int laker_get_variant(int which);
 int laker_attn_matvec_f32_noalloc(const float* rows32, int64_t m, const float* cols32, int64_t n,
                                   int d, float lam, int clamp, const float* x, float* y,
                                   void* stream);
+
+/* Device status word of the last laker_attn_matvec_f32_noalloc call on the
+ * current device (the word lives in the fixed scratch array): synchronises
+ * `stream` and writes LAKER_OK or LAKER_ERR_TIMEOUT to *status; a failed call
+ * wrote NaN to y.  It allocates nothing.  Like the entry point it reports on,
+ * it has no counterpart in the reference. */
+int laker_noalloc_status(int* status, void* stream);
 
 /* FP64 fused matvec / residual ("accurate" operator: FP64 logits, FP64 exp,
  * FP64 accumulation).
@@ -213,7 +244,8 @@ typedef struct laker_precond {
 
 size_t laker_precond_workspace_bytes(int64_t n, int nr, int k);
 
-/* Z = P R = c^-1/2 R + Q W Q^T R for R (n x k), FP64 in, FP32 or FP64 out.
+/* Z = P R = c^-1/2 R + Q W Q^T R for R (n x k), FP64 in, FP32 or FP64 out
+ * (k > 1: ldr = ldz = k).
  * Replaces preconditioner_apply_core / CCCPPreconditioner.apply
  * (laker/preconditioner.py:52-68, :286-310). */
 int laker_precond_apply(const laker_precond* pc, const double* R, int k, int64_t ldr, void* Z,
@@ -242,6 +274,11 @@ typedef struct laker_pcg_params {
   int check_every;       /* host polls the device status every N iterations */
   int has_x0;            /* 1: X holds the initial guess on entry           */
   int profile;           /* 1: time the fused matvec launches with events   */
+  int column_stop;       /* k > 1 only.  0: stop when ||B - A X||_F <= tol
+                            ||B||_F (the reference's global test); 1: each
+                            column stops on its own FP64 residual
+                            ||b_c - A x_c|| <= tol ||b_c|| and is frozen,
+                            the solve ends when every column has          */
 } laker_pcg_params;
 
 typedef struct laker_pcg_result {
@@ -260,21 +297,24 @@ typedef struct laker_pcg_result {
 
 size_t laker_pcg_workspace_bytes(int64_t n, int d, int nr, int k);
 
-/* Solves A x = b (n right-hand-side values, k = 1) with mixed-precision PCG:
- * FP32 fused operator inside the iteration, FP64 vectors, inner products and
- * scalars on the device, and reliable updates that replace the recurrence
- * residual by the FP64 residual b - A x; the stop test is on that FP64
- * residual.  k != 1 returns LAKER_ERR_UNSUPPORTED (the batched-RHS
- * recurrence of solve_2d runs in the Python layer over
- * laker_attn_matvec_f32 / _f64).  `pc` may be NULL (identity
- * preconditioner).  Every decision of an iteration is taken on the device;
- * the call captures one iteration as a CUDA graph on a private stream,
- * replays it on `stream`, polls the device state every check_every
- * iterations (0: about every 10 ms of work) and returns when the solve has
- * ended (so it cannot itself be captured into a caller's graph).  With
- * `profile` the kernels are launched one by one and the operator launches
- * timed.  Replaces PreconditionedConjugateGradient.solve / solve_1d
- * (laker/solvers.py:130-295). */
+/* Solves A X = B for k right-hand sides (B, X: n x k row-major, ld = k) with
+ * mixed-precision PCG: FP32 fused operator inside the iteration (k = 1: the
+ * symmetric single-RHS kernels; k > 1: the multi-RHS operator), FP64
+ * vectors, inner products and scalars on the device, and reliable updates
+ * that replace the recurrence residual by the FP64 residual B - A X; the stop
+ * test is on that FP64 residual.  For k > 1 alpha and beta are per column,
+ * a breakdown in any column ends the solve, and the stop test is the
+ * Frobenius one of solve_2d unless params->column_stop asks for per-column
+ * stops.  `pc` may be NULL (identity preconditioner).  Every decision of an
+ * iteration is taken on the device; the call captures one iteration as a
+ * CUDA graph on a private stream, replays it on `stream`, polls the device
+ * state every check_every iterations (0: about every 10 ms of work) and
+ * returns when the solve has ended (so it cannot itself be captured into a
+ * caller's graph).  With `profile` (k = 1) the kernels are launched one by
+ * one and the operator launches timed.  A device-side failure of a kernel
+ * (LAKER_ERR_TIMEOUT) ends the solve and is returned.  Replaces
+ * PreconditionedConjugateGradient.solve / solve_1d / solve_2d
+ * (laker/solvers.py:130-394). */
 int laker_pcg_solve(const laker_operator* op, const laker_precond* pc, const double* B, int k,
                     double* X, const laker_pcg_params* params, void* workspace,
                     size_t workspace_bytes, laker_pcg_result* result, void* stream);

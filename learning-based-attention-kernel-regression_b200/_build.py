@@ -11,6 +11,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG_DIR = Path(__file__).resolve().parent
@@ -50,28 +51,12 @@ def _stale() -> bool:
     return any(p.stat().st_mtime > lib_mtime for p in deps)
 
 
-def build(force: bool = False, verbose: bool = False, extra_flags: list[str] | None = None) -> Path:
-    """Compile every CUDA source of the package into liblaker_b200.so."""
-    if not force and not _stale():
-        return LIB_PATH
-    tmp = LIB_PATH.with_suffix(".so.tmp")
-    cmd = [
-        nvcc_path(),
-        *ARCH_FLAGS,
-        "-O3",
-        "-lineinfo",
-        "-std=c++17",
-        "--expt-relaxed-constexpr",
-        "-Xcompiler",
-        "-fPIC",
-        "-shared",
-        f"-I{INCLUDE}",
-        "-o",
-        str(tmp),
-        *[str(s) for s in sources()],
-    ]
-    if extra_flags:
-        cmd[1:1] = list(extra_flags)
+def _compile_flags() -> list[str]:
+    return [*ARCH_FLAGS, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
+            "-Xcompiler", "-fPIC", f"-I{INCLUDE}"]
+
+
+def _run(cmd: list[str], verbose: bool) -> subprocess.CompletedProcess:
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     proc = subprocess.run(cmd, capture_output=True, text=True)
@@ -79,6 +64,32 @@ def build(force: bool = False, verbose: bool = False, extra_flags: list[str] | N
         raise RuntimeError(f"nvcc failed ({proc.returncode}):\n{proc.stdout}\n{proc.stderr}")
     if verbose and (proc.stdout or proc.stderr):
         print(proc.stdout, proc.stderr, file=sys.stderr)
+    return proc
+
+
+def build(force: bool = False, verbose: bool = False, extra_flags: list[str] | None = None) -> Path:
+    """Compile every CUDA source of the package into liblaker_b200.so.
+
+    Each translation unit is compiled to an object file in parallel (no
+    relocatable device code: every unit carries its own kernels), then the
+    objects are linked into the shared library.
+    """
+    if not force and not _stale():
+        return LIB_PATH
+    flags = list(extra_flags or []) + _compile_flags()
+    objdir = PKG_DIR / "_build"
+    objdir.mkdir(exist_ok=True)
+    nvcc = nvcc_path()
+    jobs = []
+    for src in sources():
+        obj = objdir / (src.stem + ".o")
+        jobs.append((obj, [nvcc, *flags, "-c", "-o", str(obj), str(src)]))
+    workers = max(1, min(len(jobs), os.cpu_count() or 1))
+    with ThreadPoolExecutor(max_workers=workers) as pool:
+        for fut in [pool.submit(_run, cmd, verbose) for _, cmd in jobs]:
+            fut.result()
+    tmp = LIB_PATH.with_suffix(".so.tmp")
+    _run([nvcc, *ARCH_FLAGS, "-shared", "-o", str(tmp), *[str(o) for o, _ in jobs]], verbose)
     os.replace(tmp, LIB_PATH)
     return LIB_PATH
 

@@ -75,6 +75,7 @@ class laker_pcg_params(ctypes.Structure):
         ("check_every", c_int),
         ("has_x0", c_int),
         ("profile", c_int),
+        ("column_stop", c_int),
     ]
 
 
@@ -160,6 +161,8 @@ _SIGNATURES = {
         c_int,
         [_P, c_int64, _P, c_int64, c_int, c_float, c_int, _P, _P, _P],
     ),
+    "laker_noalloc_status": (c_int, [POINTER(c_int), _P]),
+    "laker_workspace_status": (c_int, [_P, POINTER(c_int), _P]),
     "laker_attn_matvec_f64": (
         c_int,
         [_P, c_int64, _P, c_int64, c_int, c_double, c_int, _P, c_int, c_int64, _P, c_int64, _P,
@@ -266,6 +269,60 @@ def workspace(nbytes: int, device: torch.device) -> torch.Tensor:
     return torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
 
 
+# Device status words of the asynchronous products, folded per (device,
+# stream) into one int32 on the device without a host synchronisation; the
+# synchronising layers (solvers, predictions, the CCCP build) read it through
+# raise_device_status.  A failed product (a bounded wait that expired on the
+# device) has also written NaN to its output.
+_pending_status: dict = {}
+
+
+def note_status(ws: torch.Tensor) -> None:
+    """Fold the status word at the start of a product's workspace into the
+    pending status of the current stream (asynchronous)."""
+    key = (ws.device.index, torch.cuda.current_stream(ws.device).cuda_stream)
+    acc = _pending_status.get(key)
+    if acc is None:
+        acc = torch.zeros(1, dtype=torch.int32, device=ws.device)
+        _pending_status[key] = acc
+    torch.maximum(acc, ws[:4].view(torch.int32), out=acc)
+
+
+def raise_device_status(device: torch.device) -> None:
+    """Raise LakerError if a product enqueued on the current stream since the
+    last check recorded a device-side failure (synchronises that stream)."""
+    device = torch.device(device)
+    if device.type != "cuda":
+        return
+    idx = device.index if device.index is not None else torch.cuda.current_device()
+    key = (idx, torch.cuda.current_stream(device).cuda_stream)
+    acc = _pending_status.get(key)
+    if acc is None:
+        return
+    v = int(acc.item())
+    if v != LAKER_OK:
+        acc.zero_()
+        raise LakerError(v, "device", status_string(v) + " (a bounded wait on the GPU expired; "
+                         "the product's outputs were written as NaN)")
+
+
+def workspace_status(ws: torch.Tensor) -> int:
+    """Status word of the last product that used `ws` (synchronises the stream)."""
+    st = c_int(0)
+    check(load().laker_workspace_status(ptr(ws), ctypes.byref(st), stream_handle(ws.device)),
+          "laker_workspace_status")
+    return int(st.value)
+
+
+def noalloc_status(device: torch.device) -> int:
+    """Status word of the last allocation-free matvec on `device`'s current
+    stream (synchronises it)."""
+    st = c_int(0)
+    check(load().laker_noalloc_status(ctypes.byref(st), stream_handle(device)),
+          "laker_noalloc_status")
+    return int(st.value)
+
+
 # ---------------------------------------------------------------------------
 # Tensor-level wrappers
 # ---------------------------------------------------------------------------
@@ -311,6 +368,7 @@ def attn_matvec_f32(rows32, m, cols32, n, d, lam, clamp, X) -> torch.Tensor:
                                   stream_handle(X.device)),
         "laker_attn_matvec_f32",
     )
+    note_status(ws)
     return Y
 
 
@@ -328,6 +386,7 @@ def attn_matvec_f64(rows64, m, cols64, n, d, lam, clamp, X, B=None) -> torch.Ten
                                   stream_handle(X.device)),
         "laker_attn_matvec_f64",
     )
+    note_status(ws)
     return Y
 
 
@@ -368,6 +427,8 @@ def precond_apply(pc: laker_precond, R: torch.Tensor, out_dtype) -> torch.Tensor
     lib = load()
     R = R.to(torch.float64).contiguous()
     k = 1 if R.dim() == 1 else R.shape[1]
+    if R.dim() == 2 and k == 1:
+        return precond_apply(pc, R[:, 0], out_dtype).unsqueeze(1)
     Z = torch.empty(R.shape, dtype=out_dtype, device=R.device)
     ws = workspace(lib.laker_precond_workspace_bytes(pc.n, pc.nr, k), R.device)
     check(
@@ -429,6 +490,7 @@ VARIANT_K2_LOGITS_N128 = 2
 VARIANT_K2_LOGITS_WIDE = 3
 VARIANT_SYM_MIN_BLOCKS = 4
 VARIANT_K1T_LOGITS = 5
+VARIANT_WAIT_LIMIT_US = 6
 
 
 def set_variant(which: int, value: int) -> int:

@@ -211,6 +211,7 @@ class LAKERCore:
         q64 = ops.pack(q, 64)
         out = ops.attn_matvec(q64, m, op.packed.packed64, op.n, op.embedding_dim, 0.0, bool(clamp),
                               alpha)
+        _lib.raise_device_status(out.device)
         out = out.to(self.dtype)
         if residual_corrector is not None:
             residual_corrector.eval()
@@ -240,5 +241,6 @@ class LAKERCore:
                                   True)
             v = pcg.solve(op.matvec, preconditioner.apply, kxq)
             var[start:end] = ops.variance_finalize(q64, end - start, d, kxq, v)
+        _lib.raise_device_status(var.device)
         self.last_pcg = pcg
         return var.to(self.dtype)

@@ -145,6 +145,18 @@ using namespace laker;
 
 extern "C" int laker_version(void) { return 100; }
 
+extern "C" int laker_workspace_status(const void* workspace, int* status, void* stream) {
+  if (!workspace || !status) return LAKER_ERR_INVALID_ARG;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int h = 0;
+  cudaError_t e = cudaMemcpyAsync(&h, &static_cast<const WsHeader*>(workspace)->status, sizeof(int),
+                                  cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fail_cuda(e);
+  *status = h;
+  return LAKER_OK;
+}
+
 extern "C" const char* laker_status_string(int status) {
   switch (status) {
     case LAKER_OK: return "ok";

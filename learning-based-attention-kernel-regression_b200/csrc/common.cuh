@@ -55,6 +55,14 @@ __device__ inline void record_status(int* status, int code) {
   if (status) atomicCAS(status, 0, code);
 }
 
+// Whether a product's status word reports a failure (its outputs are then
+// written as NaN).
+__device__ __forceinline__ bool status_failed(const int* status) {
+  return status && *const_cast<volatile const int*>(status) != 0;
+}
+__device__ __forceinline__ float nan_f32() { return __int_as_float(0x7fc00000); }
+__device__ __forceinline__ double nan_f64() { return __longlong_as_double(0x7ff8000000000000ll); }
+
 // ---------------------------------------------------------------------------
 // Fast exp2 on the MUFU pipe (PTX ex2.approx, flush-to-zero).
 // ---------------------------------------------------------------------------
@@ -113,17 +121,52 @@ __device__ __forceinline__ uint64_t global_timer_ns() {
   return t;
 }
 
+// Time limit of the bounded waits in the pipelines' loops (ns).  Each
+// translation unit has its own copy (the library is built without relocatable
+// device code); laker_set_variant(LAKER_VARIANT_WAIT_LIMIT_US, ...) sets every
+// unit's copy on the current device.  A limit of 0 makes every pipeline wait
+// give up at once, without polling: the failure path (record the status,
+// drain, return) then runs deterministically, with no fault and no hang.
+static __constant__ unsigned long long c_wait_limit_ns = 2000000000ull;
+// Drains after a failure (copies and MMAs still in flight) always get the
+// full limit: a CTA must not exit while the copy engine or the tensor core may
+// still write its shared memory.
+constexpr unsigned long long kDrainLimitNs = 2000000000ull;
+
+__device__ __forceinline__ unsigned long long wait_limit_ns() { return c_wait_limit_ns; }
+
+// Sets this translation unit's wait limit on the current device.
+[[maybe_unused]] static cudaError_t set_wait_limit_this_unit(unsigned long long ns) {
+  return cudaMemcpyToSymbol(c_wait_limit_ns, &ns, sizeof(ns));
+}
+
 // Bounded wait on an mbarrier phase.  Returns false (and records
-// LAKER_ERR_TIMEOUT) if the phase did not complete within ~2 s.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* status) {
+// LAKER_ERR_TIMEOUT) if the phase did not complete within `limit` ns, or at
+// once for a limit of 0.
+__device__ __forceinline__ bool mbar_wait_for(uint64_t* bar, uint32_t parity, int* status,
+                                              unsigned long long limit) {
+  if (limit == 0) {
+    record_status(status, LAKER_ERR_TIMEOUT);
+    return false;
+  }
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_timer_ns();
   for (uint32_t it = 0; it < (1u << 30); ++it) {
     if (mbar_try_wait(bar, parity)) return true;
-    if ((it & 255u) == 0 && global_timer_ns() - t0 > 2000000000ull) break;
+    if ((it & 255u) == 0 && global_timer_ns() - t0 >= limit) break;
   }
   record_status(status, LAKER_ERR_TIMEOUT);
   return false;
+}
+
+// A pipeline wait (the configurable limit, ~2 s by default).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* status) {
+  return mbar_wait_for(bar, parity, status, wait_limit_ns());
+}
+
+// A drain wait after a failure (always the full limit).
+__device__ __forceinline__ bool mbar_wait_drain(uint64_t* bar, uint32_t parity, int* status) {
+  return mbar_wait_for(bar, parity, status, kDrainLimitNs);
 }
 
 // ---------------------------------------------------------------------------

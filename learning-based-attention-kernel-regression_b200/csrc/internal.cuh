@@ -47,11 +47,12 @@ cudaError_t launch_k4(const double* rows64, int64_t m, const double* cols64, int
 // Y[i, :] = lam * X[i, :] (if m == n) + sum_j exp(er_i . ec_j) X[j, :]
 cudaError_t launch_multi_f32(const float* rows32, int64_t m, const float* cols32, int64_t n, int d,
                              float lam, int clamp, const float* X, int k, int64_t ldx, float* Y,
-                             int64_t ldy, cudaStream_t s);
+                             int64_t ldy, cudaStream_t s, const int* gate = nullptr);
 // Y = B - (lam X + K X) when B != nullptr, else lam X + K X (FP64 throughout).
 cudaError_t launch_multi_f64(const double* rows64, int64_t m, const double* cols64, int64_t n, int d,
                              double lam, int clamp, const double* X, int k, int64_t ldx,
-                             const double* B, int64_t ldb, double* Y, int64_t ldy, cudaStream_t s);
+                             const double* B, int64_t ldb, double* Y, int64_t ldy, cudaStream_t s,
+                             const int* gate = nullptr);
 
 // Tensor-core (tcgen05, split TF32) multi-RHS FP32 matvec (matvec_tc.cu).
 int k2_chunk_cols(int k);
@@ -59,9 +60,35 @@ size_t k2_image_bytes(int64_t m, int64_t n, int k);
 bool k2_use_tensor_cores();
 cudaError_t launch_k2(const float* rows32, int64_t m, const float* cols32, int64_t n, int d,
                       int clamp, float lam, const float* X, int64_t ldx, int k, float* Y,
-                      int64_t ldy, uint8_t* img, int* status, cudaStream_t s);
+                      int64_t ldy, uint8_t* img, int* status, cudaStream_t s,
+                      const int* gate = nullptr);
+
+// ---- multi-RHS solve and preconditioner apply (pcg_multi.cu) ----------------
+size_t pcg_multi_workspace_bytes(int64_t n, int d, int nr, int k);
+int pcg_solve_multi(const laker_operator* op, const laker_precond* pc, const double* B, int k,
+                    double* X, const laker_pcg_params* prm, void* workspace, laker_pcg_result* res,
+                    cudaStream_t s);
+// Scratch of one multi-RHS apply Z = c^-1/2 R + Q W Q^T R (R, Z: n x k).
+size_t precond_multi_scratch_bytes(int64_t n, int nr, int k);
+template <typename ZT>
+cudaError_t launch_precond_multi(const laker_precond* pc, const double* R, int k, ZT* Z,
+                                 void* scratch, const int* gate, cudaStream_t s);
 
 // Current kernel variant choice (variants.cu; LAKER_VARIANT_* in the header).
 int variant_get(int which);
+
+// Bounded-wait limit (ns) of the kernels of each translation unit that has
+// pipeline waits, on the current device (LAKER_VARIANT_WAIT_LIMIT_US).
+cudaError_t set_wait_limit_f32(unsigned long long ns);
+cudaError_t set_wait_limit_f64(unsigned long long ns);
+cudaError_t set_wait_limit_sym(unsigned long long ns);
+cudaError_t set_wait_limit_symtc(unsigned long long ns);
+cudaError_t set_wait_limit_tc(unsigned long long ns);
+
+// Y[i, c] = NaN for i < m, c < k when *status != 0: the outputs of a product
+// whose kernel recorded a device-side failure (a bounded wait that expired)
+// never look like a result.
+cudaError_t launch_poison_on_status(const int* status, float* Y, int64_t m, int k, int64_t ldy,
+                                    cudaStream_t s);
 
 }  // namespace laker

@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(T, 2)
 
   if (consumed < ntiles) {
     // A wait expired: drain (bounded) any copy still in flight, then leave.
-    for (int t = consumed + 1; t < issued; ++t) mbar_wait_bounded(&bar[t & 1], (t >> 1) & 1, status);
+    for (int t = consumed; t < issued; ++t) mbar_wait_drain(&bar[t & 1], (t >> 1) & 1, status);
     return;
   }
 
@@ -257,7 +257,9 @@ __global__ void __launch_bounds__((kMBM / 4) * (BN / 4))
     multi_matvec_kernel(const Real* __restrict__ rows, int64_t m, const Real* __restrict__ cols,
                         int64_t n, int col_layout_pairs, Real lam, const Real* __restrict__ X,
                         int k, int64_t ldx, const Real* __restrict__ B, int64_t ldb,
-                        Real* __restrict__ Y, int64_t ldy, int row_layout_pairs) {
+                        Real* __restrict__ Y, int64_t ldy, int row_layout_pairs,
+                        const int* gate) {
+  if (gate && *gate == 0) return;
   constexpr int T = (kMBM / 4) * (BN / 4);  // threads: one 4 x 4 microtile each
   static_assert(T % kMBM == 0 && (kMBM * kMBK) % T == 0, "tile / thread mapping");
   __shared__ __align__(16) Real sCol[kMBK][DP + 1];
@@ -363,42 +365,43 @@ namespace {
 template <int DP, bool CLAMP>
 cudaError_t launch_multi_f32_t(const float* rows, int64_t m, const float* cols, int64_t n, float lam,
                                const float* X, int k, int64_t ldx, float* Y, int64_t ldy,
-                               cudaStream_t s) {
+                               cudaStream_t s, const int* gate) {
   if (k <= kMBNNarrow && multi_narrow_enabled()) {
     dim3 grid((unsigned)ceil_div(m, kMBM), 1);
     multi_matvec_kernel<float, DP, CLAMP, false, kMBNNarrow>
         <<<grid, (kMBM / 4) * (kMBNNarrow / 4), 0, s>>>(rows, m, cols, n, 1, lam, X, k, ldx, nullptr,
-                                                        0, Y, ldy, 1);
+                                                        0, Y, ldy, 1, gate);
     return cudaGetLastError();
   }
   dim3 grid((unsigned)ceil_div(m, kMBM), (unsigned)ceil_div(k, kMBN));
   multi_matvec_kernel<float, DP, CLAMP, false><<<grid, kMThreads, 0, s>>>(
-      rows, m, cols, n, 1, lam, X, k, ldx, nullptr, 0, Y, ldy, 1);
+      rows, m, cols, n, 1, lam, X, k, ldx, nullptr, 0, Y, ldy, 1, gate);
   return cudaGetLastError();
 }
 
 template <int DP, bool CLAMP>
 cudaError_t launch_multi_f64_t(const double* rows, int64_t m, const double* cols, int64_t n,
                                double lam, const double* X, int k, int64_t ldx, const double* B,
-                               int64_t ldb, double* Y, int64_t ldy, cudaStream_t s) {
+                               int64_t ldb, double* Y, int64_t ldy, cudaStream_t s,
+                               const int* gate) {
   if (k <= kMBNNarrow && multi_narrow_enabled()) {
     dim3 grid((unsigned)ceil_div(m, kMBM), 1);
     constexpr int T = (kMBM / 4) * (kMBNNarrow / 4);
     if (B)
       multi_matvec_kernel<double, DP, CLAMP, true, kMBNNarrow><<<grid, T, 0, s>>>(
-          rows, m, cols, n, 0, lam, X, k, ldx, B, ldb, Y, ldy, 0);
+          rows, m, cols, n, 0, lam, X, k, ldx, B, ldb, Y, ldy, 0, gate);
     else
       multi_matvec_kernel<double, DP, CLAMP, false, kMBNNarrow><<<grid, T, 0, s>>>(
-          rows, m, cols, n, 0, lam, X, k, ldx, nullptr, 0, Y, ldy, 0);
+          rows, m, cols, n, 0, lam, X, k, ldx, nullptr, 0, Y, ldy, 0, gate);
     return cudaGetLastError();
   }
   dim3 grid((unsigned)ceil_div(m, kMBM), (unsigned)ceil_div(k, kMBN));
   if (B)
     multi_matvec_kernel<double, DP, CLAMP, true><<<grid, kMThreads, 0, s>>>(
-        rows, m, cols, n, 0, lam, X, k, ldx, B, ldb, Y, ldy, 0);
+        rows, m, cols, n, 0, lam, X, k, ldx, B, ldb, Y, ldy, 0, gate);
   else
     multi_matvec_kernel<double, DP, CLAMP, false><<<grid, kMThreads, 0, s>>>(
-        rows, m, cols, n, 0, lam, X, k, ldx, nullptr, 0, Y, ldy, 0);
+        rows, m, cols, n, 0, lam, X, k, ldx, nullptr, 0, Y, ldy, 0, gate);
   return cudaGetLastError();
 }
 
@@ -418,13 +421,23 @@ cudaError_t launch_multi_f64_t(const double* rows, int64_t m, const double* cols
 
 __global__ void finish_f32_kernel(const double* __restrict__ part, int S, int64_t m, float lam,
                                   const float* __restrict__ x, int64_t ldx, float* __restrict__ y,
-                                  int64_t ldy, int square) {
+                                  int64_t ldy, int square, const int* status) {
+  const bool failed = status_failed(status);
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
        i += (int64_t)gridDim.x * blockDim.x) {
     double acc = square ? (double)lam * (double)x[i * ldx] : 0.0;
     for (int s = 0; s < S; ++s) acc += part[(int64_t)s * m + i];
-    y[i * ldy] = (float)acc;
+    y[i * ldy] = failed ? nan_f32() : (float)acc;
   }
+}
+
+__global__ void poison_on_status_kernel(const int* __restrict__ status, float* __restrict__ Y,
+                                        int64_t m, int k, int64_t ldy) {
+  if (!status_failed(status)) return;
+  const int64_t total = m * (int64_t)k;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x)
+    Y[(t / k) * ldy + t % k] = nan_f32();
 }
 
 }  // namespace
@@ -452,28 +465,40 @@ cudaError_t launch_k1(const float* rows32, int64_t m, const float* cols32, int64
 
 cudaError_t launch_multi_f32(const float* rows32, int64_t m, const float* cols32, int64_t n, int d,
                              float lam, int clamp, const float* X, int k, int64_t ldx, float* Y,
-                             int64_t ldy, cudaStream_t s) {
+                             int64_t ldy, cudaStream_t s, const int* gate) {
   if (ceil_div(k, kMBN) > 65535) return cudaErrorInvalidValue;
   const int dp = padded_dim(d);
   if (clamp) {
-    LAKER_DISPATCH_DP(dp, return (launch_multi_f32_t<DPv, true>(rows32, m, cols32, n, lam, X, k, ldx, Y, ldy, s)));
+    LAKER_DISPATCH_DP(dp, return (launch_multi_f32_t<DPv, true>(rows32, m, cols32, n, lam, X, k, ldx, Y, ldy, s, gate)));
   } else {
-    LAKER_DISPATCH_DP(dp, return (launch_multi_f32_t<DPv, false>(rows32, m, cols32, n, lam, X, k, ldx, Y, ldy, s)));
+    LAKER_DISPATCH_DP(dp, return (launch_multi_f32_t<DPv, false>(rows32, m, cols32, n, lam, X, k, ldx, Y, ldy, s, gate)));
   }
   return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_multi_f64(const double* rows64, int64_t m, const double* cols64, int64_t n, int d,
                              double lam, int clamp, const double* X, int k, int64_t ldx,
-                             const double* B, int64_t ldb, double* Y, int64_t ldy, cudaStream_t s) {
+                             const double* B, int64_t ldb, double* Y, int64_t ldy, cudaStream_t s,
+                             const int* gate) {
   if (ceil_div(k, kMBN) > 65535) return cudaErrorInvalidValue;
   const int dp = padded_dim(d);
   if (clamp) {
-    LAKER_DISPATCH_DP(dp, return (launch_multi_f64_t<DPv, true>(rows64, m, cols64, n, lam, X, k, ldx, B, ldb, Y, ldy, s)));
+    LAKER_DISPATCH_DP(dp, return (launch_multi_f64_t<DPv, true>(rows64, m, cols64, n, lam, X, k, ldx, B, ldb, Y, ldy, s, gate)));
   } else {
-    LAKER_DISPATCH_DP(dp, return (launch_multi_f64_t<DPv, false>(rows64, m, cols64, n, lam, X, k, ldx, B, ldb, Y, ldy, s)));
+    LAKER_DISPATCH_DP(dp, return (launch_multi_f64_t<DPv, false>(rows64, m, cols64, n, lam, X, k, ldx, B, ldb, Y, ldy, s, gate)));
   }
   return cudaErrorInvalidValue;
+}
+
+cudaError_t set_wait_limit_f32(unsigned long long ns) { return set_wait_limit_this_unit(ns); }
+
+cudaError_t launch_poison_on_status(const int* status, float* Y, int64_t m, int k, int64_t ldy,
+                                    cudaStream_t s) {
+  if (m <= 0 || k <= 0) return cudaSuccess;
+  int g = (int)ceil_div(m * (int64_t)k, 256);
+  if (g > sm_count() * 4) g = sm_count() * 4;
+  poison_on_status_kernel<<<g, 256, 0, s>>>(status, Y, m, k, ldy);
+  return cudaGetLastError();
 }
 
 }  // namespace laker
@@ -517,6 +542,7 @@ extern "C" int laker_attn_matvec_f32(const float* rows32, int64_t m, const float
       uint8_t* img = reinterpret_cast<uint8_t*>(workspace) + kWsHeader;
       e = launch_k2(rows32, m, cols32, n, d, clamp, (m == n) ? lam : 0.0f, X, ldx, k, Y, ldy, img,
                     &hdr->status, s);
+      if (e == cudaSuccess) e = launch_poison_on_status(&hdr->status, Y, m, k, ldy, s);
     } else {
       e = launch_multi_f32(rows32, m, cols32, n, d, (m == n) ? lam : 0.0f, clamp, X, k, ldx, Y, ldy, s);
     }
@@ -540,7 +566,8 @@ extern "C" int laker_attn_matvec_f32(const float* rows32, int64_t m, const float
     } else {
       e = launch_k1s(cols32, n, d, clamp, X, rowpart, colpart, sp, &hdr->status, nullptr, s);
     }
-    if (e == cudaSuccess) e = launch_sym_finish(sp, rowpart, colpart, n, lam, X, Y, ldy, s);
+    if (e == cudaSuccess)
+      e = launch_sym_finish(sp, rowpart, colpart, n, lam, X, Y, ldy, &hdr->status, s);
     return e == cudaSuccess ? LAKER_OK : fail_cuda(e);
   }
   const SegPlan plan = k1_plan(m, n, d);
@@ -552,7 +579,8 @@ extern "C" int laker_attn_matvec_f32(const float* rows32, int64_t m, const float
   const int S = n > 0 ? plan.S : 0;
   int g = (int)ceil_div(m, 256);
   if (g > sm_count() * 8) g = sm_count() * 8;
-  finish_f32_kernel<<<g, 256, 0, s>>>(part, S, m, lam, X, ldx, Y, ldy, (m == n) ? 1 : 0);
+  finish_f32_kernel<<<g, 256, 0, s>>>(part, S, m, lam, X, ldx, Y, ldy, (m == n) ? 1 : 0,
+                                      &hdr->status);
   e = cudaGetLastError();
   return e == cudaSuccess ? LAKER_OK : fail_cuda(e);
 }

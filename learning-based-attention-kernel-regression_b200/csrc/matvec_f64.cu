@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(T, 2)
   }
 
   if (consumed < ntiles) {
-    for (int t = consumed + 1; t < issued; ++t) mbar_wait_bounded(&bar[t & 1], (t >> 1) & 1, status);
+    for (int t = consumed; t < issued; ++t) mbar_wait_drain(&bar[t & 1], (t >> 1) & 1, status);
     return;
   }
 #pragma unroll
@@ -141,12 +141,14 @@ cudaError_t launch_k4_t(const double* rows, int64_t m, const double* cols, int64
 __global__ void finish_f64_kernel(const double* __restrict__ part, int S, int64_t m, double lam,
                                   const double* __restrict__ x, int64_t ldx,
                                   const double* __restrict__ b, int64_t ldb,
-                                  double* __restrict__ y, int64_t ldy, int square) {
+                                  double* __restrict__ y, int64_t ldy, int square,
+                                  const int* status) {
+  const bool failed = status_failed(status);
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
        i += (int64_t)gridDim.x * blockDim.x) {
     double acc = square ? lam * x[i * ldx] : 0.0;
     for (int s = 0; s < S; ++s) acc += part[(int64_t)s * m + i];
-    y[i * ldy] = b ? b[i * ldb] - acc : acc;
+    y[i * ldy] = failed ? nan_f64() : (b ? b[i * ldb] - acc : acc);
   }
 }
 
@@ -190,6 +192,8 @@ cudaError_t launch_k4(const double* rows64, int64_t m, const double* cols64, int
   return cudaErrorInvalidValue;
 }
 
+cudaError_t set_wait_limit_f64(unsigned long long ns) { return set_wait_limit_this_unit(ns); }
+
 }  // namespace laker
 
 using namespace laker;
@@ -221,7 +225,8 @@ extern "C" int laker_attn_matvec_f64(const double* rows64, int64_t m, const doub
     double* rowpart = reinterpret_cast<double*>(wbase);
     double* colpart = sym_colpart_ptr<double>(wbase, sp);
     e = launch_k4s(rows64, n, d, clamp, X, rowpart, colpart, sp, &hdr->status, nullptr, s);
-    if (e == cudaSuccess) e = launch_sym_finish64(sp, rowpart, colpart, n, lam, X, B, ldb, Y, ldy, s);
+    if (e == cudaSuccess)
+      e = launch_sym_finish64(sp, rowpart, colpart, n, lam, X, B, ldb, Y, ldy, &hdr->status, s);
     return e == cudaSuccess ? LAKER_OK : fail_cuda(e);
   }
   const SegPlan plan = k4_plan(m, n, d);
@@ -234,7 +239,7 @@ extern "C" int laker_attn_matvec_f64(const double* rows64, int64_t m, const doub
   int g = (int)ceil_div(m, 256);
   if (g > sm_count() * 8) g = sm_count() * 8;
   finish_f64_kernel<<<g, 256, 0, s>>>(part, n > 0 ? plan.S : 0, m, lam, X, ldx, B, ldb, Y, ldy,
-                                      (m == n) ? 1 : 0);
+                                      (m == n) ? 1 : 0, &hdr->status);
   e = cudaGetLastError();
   return e == cudaSuccess ? LAKER_OK : fail_cuda(e);
 }

@@ -330,7 +330,7 @@ __global__ void __launch_bounds__(T, 3)
     if (have_nx) have_nx = cursor_next<BATCHED, B, TC, TPB>(nx, sp, bm, n);
   }
   if (failed) {
-    for (int k = consumed + 1; k < issued; ++k) mbar_wait_bounded(&bar[k & 1], (k >> 1) & 1, status);
+    for (int k = consumed; k < issued; ++k) mbar_wait_drain(&bar[k & 1], (k >> 1) & 1, status);
   }
 }
 
@@ -508,7 +508,7 @@ __global__ void __launch_bounds__(T, 1)
     if (have_nx) have_nx = cursor_next<BATCHED, B, TC, TPB>(nx, sp, bm, n);
   }
   if (failed) {
-    for (int k = consumed + 1; k < issued; ++k) mbar_wait_bounded(&bar[k & 1], (k >> 1) & 1, status);
+    for (int k = consumed; k < issued; ++k) mbar_wait_drain(&bar[k & 1], (k >> 1) & 1, status);
   }
 }
 
@@ -603,21 +603,26 @@ int k4s_occupancy(int dp) {
 
 __global__ void sym_finish_kernel(SymPlan sp, const double* __restrict__ rowpart,
                                   const float* __restrict__ colpart, int64_t n, float lam,
-                                  const float* __restrict__ x, float* __restrict__ y, int64_t ldy) {
+                                  const float* __restrict__ x, float* __restrict__ y, int64_t ldy,
+                                  const int* status) {
+  const bool failed = status_failed(status);
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
-    y[i * ldy] = (float)((double)lam * (double)x[i] + sym_row_sum(sp, rowpart, colpart, i));
+    y[i * ldy] = failed ? nan_f32()
+                        : (float)((double)lam * (double)x[i] + sym_row_sum(sp, rowpart, colpart, i));
 }
 
 // y = [b -] (lam x + K64 x) from the FP64 kernel's partials.
 __global__ void sym_finish64_kernel(SymPlan sp, const double* __restrict__ rowpart,
                                     const double* __restrict__ colpart, int64_t n, double lam,
                                     const double* __restrict__ x, const double* __restrict__ b,
-                                    int64_t ldb, double* __restrict__ y, int64_t ldy) {
+                                    int64_t ldb, double* __restrict__ y, int64_t ldy,
+                                    const int* status) {
+  const bool failed = status_failed(status);
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const double a = lam * x[i] + sym_row_sum(sp, rowpart, colpart, i);
-    y[i * ldy] = b ? b[i * ldb] - a : a;
+    y[i * ldy] = failed ? nan_f64() : (b ? b[i * ldb] - a : a);
   }
 }
 
@@ -671,10 +676,10 @@ cudaError_t launch_k1s_batched(const float* E32, int d, int clamp, const float* 
 
 cudaError_t launch_sym_finish(const SymPlan& sp, const double* rowpart, const float* colpart,
                               int64_t n, float lam, const float* x, float* y, int64_t ldy,
-                              cudaStream_t s) {
+                              const int* status, cudaStream_t s) {
   int g = (int)ceil_div(n, 256);
   if (g > sm_count() * 8) g = sm_count() * 8;
-  sym_finish_kernel<<<g, 256, 0, s>>>(sp, rowpart, colpart, n, lam, x, y, ldy);
+  sym_finish_kernel<<<g, 256, 0, s>>>(sp, rowpart, colpart, n, lam, x, y, ldy, status);
   return cudaGetLastError();
 }
 
@@ -724,12 +729,15 @@ cudaError_t launch_k4s_batched(const double* E64, int d, int clamp, const double
 
 cudaError_t launch_sym_finish64(const SymPlan& sp, const double* rowpart, const double* colpart,
                                 int64_t n, double lam, const double* x, const double* b,
-                                int64_t ldb, double* y, int64_t ldy, cudaStream_t s) {
+                                int64_t ldb, double* y, int64_t ldy, const int* status,
+                                cudaStream_t s) {
   int g = (int)ceil_div(n, 256);
   if (g > sm_count() * 8) g = sm_count() * 8;
-  sym_finish64_kernel<<<g, 256, 0, s>>>(sp, rowpart, colpart, n, lam, x, b, ldb, y, ldy);
+  sym_finish64_kernel<<<g, 256, 0, s>>>(sp, rowpart, colpart, n, lam, x, b, ldb, y, ldy, status);
   return cudaGetLastError();
 }
+
+cudaError_t set_wait_limit_sym(unsigned long long ns) { return set_wait_limit_this_unit(ns); }
 
 // Square operators of at most LAKER_VARIANT_SYM_MIN_BLOCKS 512-point blocks
 // (default 6: n <= 3072, at most 21 block pairs, so as many CTAs) run the

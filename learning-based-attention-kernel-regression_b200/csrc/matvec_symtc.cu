@@ -579,13 +579,13 @@ __global__ void __launch_bounds__(kTThreads, 1)
   if (*abort) {
     // bounded drains of the copies in flight and of the MMAs issued
     if (warp == kTCopyWarp && lane == 0) {
-      if (a_issued > 0) mbar_wait_bounded(a_full, (uint32_t)((a_issued - 1) & 1), status);
+      if (a_issued > 0) mbar_wait_drain(a_full, (uint32_t)((a_issued - 1) & 1), status);
       for (int64_t gg = b_issued > 2 ? b_issued - 2 : 0; gg < b_issued; ++gg)
-        mbar_wait_bounded(&b_full[gg & 1], (uint32_t)((gg >> 1) & 1), status);
+        mbar_wait_drain(&b_full[gg & 1], (uint32_t)((gg >> 1) & 1), status);
     }
     if (warp == kTMmaWarp && lane == 0 && mma_any) {
       mma_commit(drain);
-      mbar_wait_bounded(drain, 0u, status);
+      mbar_wait_drain(drain, 0u, status);
     }
   }
   tc_fence_before();
@@ -700,5 +700,7 @@ cudaError_t launch_k1t_batched(const uint8_t* img, int clamp, const float* x, do
   return clamp ? launch_k1t_ut<true, true>(img, 0, x, rowpart, colpart, sp, bm, status, gate, s, fmt)
                : launch_k1t_ut<false, true>(img, 0, x, rowpart, colpart, sp, bm, status, gate, s, fmt);
 }
+
+cudaError_t set_wait_limit_symtc(unsigned long long ns) { return set_wait_limit_this_unit(ns); }
 
 }  // namespace laker

@@ -72,7 +72,8 @@ __host__ __device__ constexpr uint32_t tf32_idesc(int n) { return tf32_idesc_mn(
 // [lo: N rows x 4 TK B], row = right-hand side, TK points per row.
 template <int TK>
 __global__ void k2_pack_x(const float* __restrict__ X, int64_t n, int64_t ldx, int k, int N,
-                          int64_t ntiles, uint8_t* __restrict__ img) {
+                          int64_t ntiles, uint8_t* __restrict__ img, const int* gate) {
+  if (gate && *gate == 0) return;
   constexpr int kTcTileK = TK;
   const int64_t total = (int64_t)ntiles * kTcTileK * ((k + N - 1) / N) * N;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
@@ -130,7 +131,8 @@ __global__ void __launch_bounds__(kTcThreadsWs, 1)
     k2_tc_matvec(const float* __restrict__ rows32, int64_t m, const float* __restrict__ cols32,
                  const uint8_t* __restrict__ img, int N, int S, K2Work wk, float lam,
                  const float* __restrict__ X, int64_t ldx, int k, float* __restrict__ Y,
-                 int64_t ldy, float* __restrict__ part, int* status) {
+                 int64_t ldy, float* __restrict__ part, int* status, const int* gate) {
+  if (gate && *gate == 0) return;
   constexpr int kABytes = TileCfg<TK>::kABytes;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -360,12 +362,12 @@ __global__ void __launch_bounds__(kTcThreadsWs, 1)
       // the latest copy of every stage (earlier ones were consumed)
       const int64_t from = b_issued > S ? b_issued - S : 0;
       for (int64_t gg = from; gg < b_issued; ++gg)
-        mbar_wait_bounded(&b_full[gg % S], (uint32_t)((gg / S) & 1), status);
+        mbar_wait_drain(&b_full[gg % S], (uint32_t)((gg / S) & 1), status);
     }
     if (warp == 9 && lane == 0 && mma_tiles > 0) {
       // the last commit completes when every MMA issued before it has
       const int64_t gg = mma_tiles - 1;
-      mbar_wait_bounded(&b_empty[gg % S], (uint32_t)((gg / S) & 1), status);
+      mbar_wait_drain(&b_empty[gg % S], (uint32_t)((gg / S) & 1), status);
     }
   }
   tc_fence_before();
@@ -398,7 +400,8 @@ __global__ void __launch_bounds__(kK2tThreads, 1)
     k2t_matvec(const uint8_t* __restrict__ rimg, int64_t m, const uint8_t* __restrict__ cimg,
                const uint8_t* __restrict__ img, int N, int S, int AS, K2Work wk, float lam,
                const float* __restrict__ X, int64_t ldx, int k, float* __restrict__ Y, int64_t ldy,
-               float* __restrict__ part, int* status) {
+               float* __restrict__ part, int* status, const int* gate) {
+  if (gate && *gate == 0) return;
   constexpr int kABytes = TileCfg<TK>::kABytes;
   constexpr uint32_t kArBytes = kTcRows * 64;   // one variant of the rows' operand
   constexpr uint32_t kBcBytes = TK * 64;        // one variant of a tile's points' operand
@@ -676,14 +679,14 @@ __global__ void __launch_bounds__(kK2tThreads, 1)
   if (*abort) {
     // bounded drains of the copies in flight and of the MMAs issued
     if (warp == kK2tCopyWarp && lane == 0) {
-      if (ar_issued > 0) mbar_wait_bounded(ar_full, (uint32_t)((ar_issued - 1) & 1), status);
+      if (ar_issued > 0) mbar_wait_drain(ar_full, (uint32_t)((ar_issued - 1) & 1), status);
       const int64_t from = b_issued > S ? b_issued - S : 0;
       for (int64_t gg = from; gg < b_issued; ++gg)
-        mbar_wait_bounded(&b_full[gg % S], (uint32_t)((gg / S) & 1), status);
+        mbar_wait_drain(&b_full[gg % S], (uint32_t)((gg / S) & 1), status);
     }
     if (warp == kK2tMmaWarp && lane == 0 && mma_any) {
       mma_commit(drain);
-      mbar_wait_bounded(drain, 0u, status);
+      mbar_wait_drain(drain, 0u, status);
     }
   }
   tc_fence_before();
@@ -697,7 +700,8 @@ __global__ void __launch_bounds__(kK2tThreads, 1)
 // Y = lam X + sum over segments of the partials, in segment order.
 __global__ void k2_reduce_kernel(const float* __restrict__ part, int segs, int64_t m, int k,
                                  float lam, const float* __restrict__ X, int64_t ldx,
-                                 float* __restrict__ Y, int64_t ldy) {
+                                 float* __restrict__ Y, int64_t ldy, const int* gate) {
+  if (gate && *gate == 0) return;
   const int64_t total = m * (int64_t)k;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
        e += (int64_t)gridDim.x * blockDim.x) {
@@ -763,7 +767,8 @@ K2Work k2_work(int64_t m, int64_t n, int k, int N, int TK) {
 template <int DP, bool CLAMP, int TK>
 cudaError_t launch_k2_t(const float* rows32, int64_t m, const float* cols32, const uint8_t* img,
                         int N, const K2Work& wk, float lam, const float* X, int64_t ldx, int k,
-                        float* Y, int64_t ldy, float* part, int* status, cudaStream_t s) {
+                        float* Y, int64_t ldy, float* part, int* status, cudaStream_t s,
+                        const int* gate) {
   const int S = k2_stages(N, TK, DP);
   const size_t smem = k2_smem_bytes(N, S, TK, DP);
   if (S < 2 || smem > 227 * 1024) return cudaErrorInvalidConfiguration;
@@ -772,19 +777,20 @@ cudaError_t launch_k2_t(const float* rows32, int64_t m, const float* cols32, con
   if (e != cudaSuccess) return e;
   const int64_t grid = wk.items < (int64_t)sm_count() ? wk.items : (int64_t)sm_count();
   fn<<<(unsigned)grid, kTcThreadsWs, smem, s>>>(rows32, m, cols32, img, N, S, wk, lam, X, ldx, k, Y,
-                                                ldy, part, status);
+                                                ldy, part, status, gate);
   return cudaGetLastError();
 }
 
 template <int DP, bool CLAMP>
 cudaError_t launch_k2_tk(const float* rows32, int64_t m, const float* cols32, const uint8_t* img,
                          int N, int TK, const K2Work& wk, float lam, const float* X, int64_t ldx,
-                         int k, float* Y, int64_t ldy, float* part, int* status, cudaStream_t s) {
+                         int k, float* Y, int64_t ldy, float* part, int* status, cudaStream_t s,
+                         const int* gate) {
   if (TK == 32)
     return launch_k2_t<DP, CLAMP, 32>(rows32, m, cols32, img, N, wk, lam, X, ldx, k, Y, ldy, part,
-                                      status, s);
+                                      status, s, gate);
   return launch_k2_t<DP, CLAMP, 16>(rows32, m, cols32, img, N, wk, lam, X, ldx, k, Y, ldy, part,
-                                    status, s);
+                                    status, s, gate);
 }
 
 // Logit-on-tensor-core variant: P slots (2 for wide chunks, 4 for narrow
@@ -808,7 +814,8 @@ size_t k2t_smem_bytes(int N, int S, int AS) {
 template <bool CLAMP>
 cudaError_t launch_k2t_t(const uint8_t* rimg, int64_t m, const uint8_t* cimg, const uint8_t* img,
                          int N, const K2Work& wk, float lam, const float* X, int64_t ldx, int k,
-                         float* Y, int64_t ldy, float* part, int* status, cudaStream_t s) {
+                         float* Y, int64_t ldy, float* part, int* status, cudaStream_t s,
+                         const int* gate) {
   const int AS = k2t_pslots(N);
   const int S = k2t_stages(N, AS);
   const size_t smem = k2t_smem_bytes(N, S, AS);
@@ -818,7 +825,7 @@ cudaError_t launch_k2t_t(const uint8_t* rimg, int64_t m, const uint8_t* cimg, co
   if (e != cudaSuccess) return e;
   const int64_t grid = wk.items < (int64_t)sm_count() ? wk.items : (int64_t)sm_count();
   fn<<<(unsigned)grid, kK2tThreads, smem, s>>>(rimg, m, cimg, img, N, S, AS, wk, lam, X, ldx, k, Y,
-                                               ldy, part, status);
+                                               ldy, part, status, gate);
   return cudaGetLastError();
 }
 
@@ -879,7 +886,7 @@ bool k2_use_tensor_cores() {
 // img: k2_image_bytes(m, n, k) of workspace.
 cudaError_t launch_k2(const float* rows32, int64_t m, const float* cols32, int64_t n, int d,
                       int clamp, float lam, const float* X, int64_t ldx, int k, float* Y,
-                      int64_t ldy, uint8_t* img, int* status, cudaStream_t s) {
+                      int64_t ldy, uint8_t* img, int* status, cudaStream_t s, const int* gate) {
   const int N = k2_chunk_cols(k);
   const int TK = k2_tk_for(N);
   const K2Work wk = k2_work(m, n, k, N, TK);
@@ -892,9 +899,9 @@ cudaError_t launch_k2(const float* rows32, int64_t m, const float* cols32, int64
     int64_t g = ceil_div(total, 256);
     if (g > (int64_t)sm_count() * 16) g = (int64_t)sm_count() * 16;
     if (TK == 32)
-      k2_pack_x<32><<<(unsigned)g, 256, 0, s>>>(X, n, ldx, k, N, wk.ntiles, img);
+      k2_pack_x<32><<<(unsigned)g, 256, 0, s>>>(X, n, ldx, k, N, wk.ntiles, img, gate);
     else
-      k2_pack_x<16><<<(unsigned)g, 256, 0, s>>>(X, n, ldx, k, N, wk.ntiles, img);
+      k2_pack_x<16><<<(unsigned)g, 256, 0, s>>>(X, n, ldx, k, N, wk.ntiles, img, gate);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
@@ -912,18 +919,20 @@ cudaError_t launch_k2(const float* rows32, int64_t m, const float* cols32, int64
       e = launch_k1t_pack(cols32, n, d, cimg, crows, s);
     }
     if (e == cudaSuccess)
-      e = clamp ? launch_k2t_t<true>(rimg, m, cimg, img, N, wk, lam, X, ldx, k, Y, ldy, part, status, s)
-                : launch_k2t_t<false>(rimg, m, cimg, img, N, wk, lam, X, ldx, k, Y, ldy, part, status, s);
+      e = clamp ? launch_k2t_t<true>(rimg, m, cimg, img, N, wk, lam, X, ldx, k, Y, ldy, part, status, s, gate)
+                : launch_k2t_t<false>(rimg, m, cimg, img, N, wk, lam, X, ldx, k, Y, ldy, part, status, s, gate);
   } else if (clamp) {
-    LAKER_DISPATCH_TC(dp, e = (launch_k2_tk<DPv, true>(rows32, m, cols32, img, N, TK, wk, lam, X, ldx, k, Y, ldy, part, status, s)));
+    LAKER_DISPATCH_TC(dp, e = (launch_k2_tk<DPv, true>(rows32, m, cols32, img, N, TK, wk, lam, X, ldx, k, Y, ldy, part, status, s, gate)));
   } else {
-    LAKER_DISPATCH_TC(dp, e = (launch_k2_tk<DPv, false>(rows32, m, cols32, img, N, TK, wk, lam, X, ldx, k, Y, ldy, part, status, s)));
+    LAKER_DISPATCH_TC(dp, e = (launch_k2_tk<DPv, false>(rows32, m, cols32, img, N, TK, wk, lam, X, ldx, k, Y, ldy, part, status, s, gate)));
   }
   if (e != cudaSuccess || wk.segs == 1) return e;
   int64_t g = ceil_div(m * (int64_t)k, 256);
   if (g > (int64_t)sm_count() * 16) g = (int64_t)sm_count() * 16;
-  k2_reduce_kernel<<<(unsigned)g, 256, 0, s>>>(part, wk.segs, m, k, lam, X, ldx, Y, ldy);
+  k2_reduce_kernel<<<(unsigned)g, 256, 0, s>>>(part, wk.segs, m, k, lam, X, ldx, Y, ldy, gate);
   return cudaGetLastError();
 }
+
+cudaError_t set_wait_limit_tc(unsigned long long ns) { return set_wait_limit_this_unit(ns); }
 
 }  // namespace laker

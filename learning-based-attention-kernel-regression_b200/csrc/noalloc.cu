@@ -19,6 +19,11 @@
 // word is cleared at the start of every call (the partials are fully
 // overwritten), and calls whose work overlaps on the GPU -- on different
 // streams, or from different host threads without ordering -- race on it.
+// A device-side failure (a bounded wait that expired) makes the call write
+// NaN to y and leaves LAKER_ERR_TIMEOUT in the status word, which
+// laker_noalloc_status reads back.  The cached address of the array is only
+// valid in the device context it was looked up in: the entry point must not
+// be used across a cudaDeviceReset.
 #include <mutex>
 
 #include "internal.cuh"
@@ -50,14 +55,18 @@ cudaError_t noalloc_scratch(void** out) {
   return cudaSuccess;
 }
 
+// y from the segment partials; NaN everywhere when the matvec kernel recorded
+// a failure (a CTA whose bounded wait expired left its partials unwritten, and
+// the array still holds the previous call's).
 __global__ void noalloc_finish_kernel(const double* __restrict__ part, int S, int64_t m, float lam,
                                       const float* __restrict__ x, float* __restrict__ y,
-                                      int square) {
+                                      int square, const int* status) {
+  const bool failed = status_failed(status);
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
        i += (int64_t)gridDim.x * blockDim.x) {
     double acc = square ? (double)lam * (double)x[i] : 0.0;
     for (int s = 0; s < S; ++s) acc += part[(int64_t)s * m + i];
-    y[i] = (float)acc;
+    y[i] = failed ? nan_f32() : (float)acc;
   }
 }
 
@@ -103,7 +112,21 @@ extern "C" int laker_attn_matvec_f32_noalloc(const float* rows32, int64_t m, con
   int g = (int)ceil_div(m, 256);
   if (g > sm_count() * 8) g = sm_count() * 8;
   noalloc_finish_kernel<<<g, 256, 0, s>>>(part, n > 0 ? plan.S : 0, m, lam, x, y,
-                                          (m == n) ? 1 : 0);
+                                          (m == n) ? 1 : 0, status);
   e = cudaGetLastError();
   return e == cudaSuccess ? LAKER_OK : fail_cuda(e);
+}
+
+extern "C" int laker_noalloc_status(int* status, void* stream) {
+  if (!status) return LAKER_ERR_INVALID_ARG;
+  void* base = nullptr;
+  cudaError_t e = noalloc_scratch(&base);
+  if (e != cudaSuccess) return fail_cuda(e);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int h = 0;
+  e = cudaMemcpyAsync(&h, base, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fail_cuda(e);
+  *status = h;
+  return LAKER_OK;
 }

@@ -83,7 +83,8 @@ __global__ void __launch_bounds__(T)
     pcg_after_matvec_kernel(const double* __restrict__ part, int S, SymPlan sp,
                             const double* __restrict__ rowpart,
                             const float* __restrict__ colpart, const float* __restrict__ p,
-                            float* __restrict__ Ap, int64_t n, double* blockpart, PcgState* st) {
+                            float* __restrict__ Ap, int64_t n, double* blockpart, PcgState* st,
+                            const int* dstatus) {
   if (st->done) return;
   __shared__ double s_red[3 * (T / 32)];
   const double lam = st->lam;
@@ -118,7 +119,13 @@ __global__ void __launch_bounds__(T)
       aa += __ldcg(blockpart + 3 * k + 2);
     }
     st->pAp = pap;
-    if (!isfinite(pap) || !isfinite(pp) || !isfinite(aa)) {
+    if (status_failed(dstatus)) {
+      // the operator kernel recorded a device-side failure: its partials are
+      // not a product
+      st->status = *dstatus;
+      st->done = 1;
+      st->active = 0;
+    } else if (!isfinite(pap) || !isfinite(pp) || !isfinite(aa)) {
       st->status = LAKER_ERR_NONFINITE;
       st->done = 1;
       st->active = 0;
@@ -387,7 +394,7 @@ using namespace laker;
 
 extern "C" size_t laker_pcg_workspace_bytes(int64_t n, int d, int nr, int k) {
   if (n < 1 || d < 1 || d > 16 || nr < 0 || nr > kMaxNr || k < 1) return 0;
-  if (k != 1) return 0;
+  if (k != 1) return pcg_multi_workspace_bytes(n, d, nr, k);
   return carve(nullptr, n, d, nr).bytes;
 }
 
@@ -396,7 +403,7 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
                                size_t workspace_bytes, laker_pcg_result* res, void* stream) {
   if (!op || !prm || !res || !B || !X || !workspace) return LAKER_ERR_INVALID_ARG;
   if (op->n < 1 || op->d < 1 || op->d > 16 || !op->packed32 || !op->packed64) return LAKER_ERR_INVALID_ARG;
-  if (k != 1) return LAKER_ERR_UNSUPPORTED;
+  if (k < 1) return LAKER_ERR_INVALID_ARG;
   if (pc && (pc->n != op->n || !precond_valid(pc))) return LAKER_ERR_INVALID_ARG;
   if (prm->max_iter < 0 || !(prm->tol >= 0.0) || !(prm->reliable_delta > 0.0)) return LAKER_ERR_INVALID_ARG;
   const int64_t n = op->n;
@@ -405,6 +412,7 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
   if (workspace_bytes < laker_pcg_workspace_bytes(n, d, nr, k)) return LAKER_ERR_WORKSPACE;
 
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (k > 1) return pcg_solve_multi(op, pc, B, k, X, prm, workspace, res, s);
   PcgWs w = carve(workspace, n, d, nr);
   const SegPlan p1 = k1_plan(n, n, d), p4 = k4_plan(n, n, d);
   const bool sym = k1_symmetric_for(n);
@@ -517,10 +525,10 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
     if (timed) t32.end(cs);
     if (sym)
       pcg_after_matvec_kernel<true><<<G, T, 0, cs>>>(w.part32, 0, sp, sym_row, sym_col, w.p, w.Ap, n,
-                                                     w.blockpart, w.st);
+                                                     w.blockpart, w.st, dstatus);
     else
       pcg_after_matvec_kernel<false><<<G, T, 0, cs>>>(w.part32, p1.S, sp, nullptr, nullptr, w.p, w.Ap,
-                                                      n, w.blockpart, w.st);
+                                                      n, w.blockpart, w.st, dstatus);
     pcg_update_xr_kernel<<<G, T, 0, cs>>>(w.p, w.Ap, X, w.r, n, w.blockpart, w.st);
     if (timed) t64.begin(cs);
     launch_residual(0, &w.st->need_update, cs);

@@ -1,0 +1,837 @@
+// Mixed-precision preconditioned conjugate gradient for k right-hand sides at
+// once (the batched-RHS solve of the predictive variance), device resident.
+//
+// Iteration, every scalar per column and on the device (solve_2d,
+// laker/solvers.py:297-394):
+//   AP = lam P + K32 P                    multi-RHS FP32 operator
+//   pAp_c, |p_c|, |Ap_c|                   -> alpha_c; breakdown if any column
+//                                             has p_c^T A p_c <= -eps |p_c| |Ap_c|
+//   X += P diag(alpha); R -= AP diag(alpha)        (X, R in FP64); |R|_F
+//   reliable update: R = B - A64 X (FP64 multi-RHS residual) when |R|_F fell
+//     by `delta` from its running maximum since the last recomputation, when
+//     the recurrence says the stop test may hold, and at max_iter; the stop
+//     test is only taken on that FP64 residual:
+//       default      |R|_F <= tol |B|_F   (the reference's global Frobenius
+//                                         test, solvers.py:365-368)
+//       column_stop  every column c with |r_c| <= tol |b_c| is frozen (its
+//                    alpha, beta and search direction become zero) and the
+//                    solve ends when all are
+//   Z = P R (factored CCCP apply, multi-RHS); rz_c -> beta_c
+//   P = Z + P diag(beta)
+// Every kernel reads the device state first and does nothing once the solve
+// has ended, so the host replays the captured iteration several times between
+// polls.  Column reductions are fixed-order (per-CTA partials over a fixed row
+// partition, then a fixed-order sum by the last CTA), so results do not depend
+// on scheduling.  Data are row-major n x k with leading dimension k.
+//
+// A column whose search direction is exactly zero (a zero right-hand side) is
+// solved exactly (x_c = 0, alpha_c = 0); the reference's breakdown test
+// reports p^T A p = 0 <= -eps * 0 as a breakdown for it instead.
+#include <chrono>
+
+#include "pcg_state.cuh"
+#include "sym.cuh"
+
+namespace laker {
+
+bool precond_valid(const laker_precond* pc);
+
+namespace {
+
+constexpr int kMT = 256;         // threads of the vector kernels
+constexpr int kCW = 32;          // columns per CTA of the column-reduction kernels
+constexpr int kRW = kMT / kCW;   // row lanes per CTA
+constexpr int kGT = 64;          // output tile (rows x columns) of the apply's GEMMs
+constexpr int kGK = 16;          // K step of the apply's GEMMs
+
+struct alignas(256) MpcgState {
+  double bnorm;       // |B|_F
+  double tol_abs;     // tol |B|_F
+  double tol;         // relative tolerance
+  double rnorm;       // |R|_F of the recurrence (after the last update)
+  double rmax;        // running max of |R|_F since the last FP64 recomputation
+  double true_rnorm;  // |B - A X|_F from the last FP64 recomputation
+  double delta;       // reliable-update factor
+  double eps;         // breakdown threshold
+  int iter;           // iterations (FP32 operator applications)
+  int n_accurate;     // FP64 residual recomputations
+  int max_iter;
+  int active;         // 1 while the solve runs (gate of the operator)
+  int need_update;    // 1 when this iteration ends with an FP64 recomputation
+  int done;
+  int status;
+  int column_stop;    // 1: per-column stop test with freezing
+  int n_live;         // columns still iterating
+  int pad;
+  unsigned int counters[8];
+};
+
+enum { kMCtrInit = 0, kMCtrMatvec, kMCtrUpdate, kMCtrResid, kMCtrPrecond };
+
+// Per-column state (k entries each), in the workspace.
+struct MpcgCols {
+  double* bnorm;  // |b_c|
+  double* rz;     // r_c . z_c
+  double* alpha;
+  double* beta;
+  double* rn;     // |r_c|: recurrence, or the FP64 residual after a recomputation
+  int* live;      // 1 while column c iterates
+};
+
+__device__ __forceinline__ void mp_stop(MpcgState* st, int status) {
+  st->status = status;
+  st->done = 1;
+  st->active = 0;
+}
+
+// Column-reduction grid: blockIdx.y covers columns [32 y, 32 y + 32),
+// blockIdx.x rows x*8 + r + gx*8*t (r = thread row lane).
+struct ColGrid {
+  int gx, gy;
+};
+
+ColGrid col_grid(int64_t n, int k) {
+  ColGrid g{};
+  g.gy = (int)ceil_div(k, kCW);
+  int64_t gx = ceil_div(2 * (int64_t)sm_count(), g.gy);
+  const int64_t lim = ceil_div(n, kRW);
+  if (gx > lim) gx = lim;
+  if (gx > 512) gx = 512;
+  g.gx = (int)(gx < 1 ? 1 : gx);
+  return g;
+}
+
+// Stores this CTA's per-column partial sums of NQ quantities (fixed order over
+// the CTA's row lanes) at bp[q * qstride + blockIdx.x * k + c].
+template <int NQ>
+__device__ __forceinline__ void store_col_partials(const double (&v)[NQ], double* bp,
+                                                   int64_t qstride, int k) {
+  __shared__ double s[NQ][kRW][kCW];
+  const int tc = threadIdx.x % kCW, tr = threadIdx.x / kCW;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) s[q][tr][tc] = v[q];
+  __syncthreads();
+  if (tr == 0) {
+    const int c = blockIdx.y * kCW + tc;
+    if (c < k) {
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        double t = 0.0;
+#pragma unroll
+        for (int r = 0; r < kRW; ++r) t += s[q][r][tc];
+        bp[q * qstride + (int64_t)blockIdx.x * k + c] = t;
+      }
+    }
+  }
+}
+
+// Fixed-order total of column c over the gx CTA partials.
+__device__ __forceinline__ double col_total(const double* bp, int gx, int k, int c) {
+  double t = 0.0;
+  for (int b = 0; b < gx; ++b) t += __ldcg(bp + (int64_t)b * k + c);
+  return t;
+}
+
+// X = 0 and R = B (unless warm start), |b_c| -> bnorm, |B|_F, tolerances.
+__global__ void __launch_bounds__(kMT)
+    mp_init_kernel(const double* __restrict__ B, double* __restrict__ X, double* __restrict__ R,
+                   int64_t n, int k, int has_x0, double* bp, MpcgState* st, MpcgCols cols) {
+  __shared__ double s_red[kMT / 32];
+  const int c = blockIdx.y * kCW + threadIdx.x % kCW;
+  double acc = 0.0;
+  if (c < k) {
+    for (int64_t i = (int64_t)blockIdx.x * kRW + threadIdx.x / kCW; i < n;
+         i += (int64_t)gridDim.x * kRW) {
+      const int64_t e = i * k + c;
+      const double b = B[e];
+      if (!has_x0) {
+        R[e] = b;
+        X[e] = 0.0;
+      }
+      acc = fma(b, b, acc);
+    }
+  }
+  const double v[1] = {acc};
+  store_col_partials<1>(v, bp, 0, k);
+  if (!arrive_last_block(&st->counters[kMCtrInit])) return;
+  double fro = 0.0;
+  for (int cc = threadIdx.x; cc < k; cc += kMT) {
+    const double t = col_total(bp, gridDim.x, k, cc);
+    const double bn = sqrt(t);
+    cols.bnorm[cc] = bn;
+    cols.rn[cc] = bn;
+    cols.live[cc] = 1;
+    fro += t;
+  }
+  double f[1] = {fro};
+  block_sum<kMT, 1>(f, s_red);
+  if (threadIdx.x == 0) {
+    const double bn = sqrt(f[0]);
+    st->bnorm = bn;
+    st->tol_abs = st->tol * bn;
+    st->rnorm = bn;
+    st->rmax = bn;
+    st->true_rnorm = bn;
+    st->n_live = k;
+    if (!isfinite(bn)) mp_stop(st, LAKER_ERR_NONFINITE);
+  }
+}
+
+// pAp_c, p_c.p_c, Ap_c.Ap_c -> alpha_c and the breakdown test.  A device-side
+// failure of the operator (its status word) ends the solve with that status.
+__global__ void __launch_bounds__(kMT)
+    mp_after_matvec_kernel(const float* __restrict__ P, const float* __restrict__ AP, int64_t n,
+                           int k, double* bp, MpcgState* st, MpcgCols cols, const int* dstatus) {
+  if (st->done) return;
+  const int c = blockIdx.y * kCW + threadIdx.x % kCW;
+  double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+  if (c < k) {
+    for (int64_t i = (int64_t)blockIdx.x * kRW + threadIdx.x / kCW; i < n;
+         i += (int64_t)gridDim.x * kRW) {
+      const double p = P[i * k + c], a = AP[i * k + c];
+      d0 = fma(p, a, d0);
+      d1 = fma(p, p, d1);
+      d2 = fma(a, a, d2);
+    }
+  }
+  const int64_t qs = (int64_t)gridDim.x * k;
+  const double v[3] = {d0, d1, d2};
+  store_col_partials<3>(v, bp, qs, k);
+  if (!arrive_last_block(&st->counters[kMCtrMatvec])) return;
+  const double eps = st->eps;
+  bool nonfinite = false, breakdown = false;
+  for (int cc = threadIdx.x; cc < k; cc += kMT) {
+    if (!cols.live[cc]) {
+      cols.alpha[cc] = 0.0;
+      continue;
+    }
+    const double pap = col_total(bp, gridDim.x, k, cc);
+    const double pp = col_total(bp + qs, gridDim.x, k, cc);
+    const double aa = col_total(bp + 2 * qs, gridDim.x, k, cc);
+    if (!isfinite(pap) || !isfinite(pp) || !isfinite(aa)) {
+      nonfinite = true;
+    } else if (pp > 0.0 && pap <= -eps * sqrt(pp) * sqrt(aa)) {
+      breakdown = true;  // non-positive curvature (laker/solvers.py:343-352)
+    }
+    cols.alpha[cc] = (pp > 0.0 && pap != 0.0) ? cols.rz[cc] / pap : 0.0;
+  }
+  const int nf = __syncthreads_or(nonfinite ? 1 : 0);
+  const int bd = __syncthreads_or(breakdown ? 1 : 0);
+  if (threadIdx.x == 0) {
+    if (status_failed(dstatus)) mp_stop(st, *dstatus);
+    else if (nf) mp_stop(st, LAKER_ERR_NONFINITE);
+    else if (bd) mp_stop(st, LAKER_ERR_BREAKDOWN);
+  }
+}
+
+// X += alpha P; R -= alpha AP; |r_c|, |R|_F -> decide on the FP64 recomputation.
+__global__ void __launch_bounds__(kMT)
+    mp_update_xr_kernel(const float* __restrict__ P, const float* __restrict__ AP,
+                        double* __restrict__ X, double* __restrict__ R, int64_t n, int k, double* bp,
+                        MpcgState* st, MpcgCols cols) {
+  if (st->done) return;
+  __shared__ double s_red[kMT / 32];
+  const int c = blockIdx.y * kCW + threadIdx.x % kCW;
+  double acc = 0.0;
+  if (c < k) {
+    const double a = cols.alpha[c];
+    for (int64_t i = (int64_t)blockIdx.x * kRW + threadIdx.x / kCW; i < n;
+         i += (int64_t)gridDim.x * kRW) {
+      const int64_t e = i * k + c;
+      X[e] = fma(a, (double)P[e], X[e]);
+      const double r = fma(-a, (double)AP[e], R[e]);
+      R[e] = r;
+      acc = fma(r, r, acc);
+    }
+  }
+  const double v[1] = {acc};
+  store_col_partials<1>(v, bp, 0, k);
+  if (!arrive_last_block(&st->counters[kMCtrUpdate])) return;
+  const double tol = st->tol;
+  double fro = 0.0;
+  bool below = true;  // every live column's recurrence residual at its tolerance
+  for (int cc = threadIdx.x; cc < k; cc += kMT) {
+    const double t = col_total(bp, gridDim.x, k, cc);
+    const double rn = sqrt(t);
+    cols.rn[cc] = rn;
+    fro += t;
+    if (cols.live[cc] && !(rn <= tol * cols.bnorm[cc])) below = false;
+  }
+  double f[1] = {fro};
+  block_sum<kMT, 1>(f, s_red);
+  const int all_below = __syncthreads_and(below ? 1 : 0);
+  if (threadIdx.x == 0) {
+    const double rn = sqrt(f[0]);
+    st->rnorm = rn;
+    st->iter += 1;
+    if (rn > st->rmax) st->rmax = rn;
+    const bool may_stop = st->column_stop ? (all_below != 0) : (rn <= st->tol_abs);
+    st->need_update =
+        (rn <= st->delta * st->rmax || may_stop || st->iter >= st->max_iter || !isfinite(rn)) ? 1 : 0;
+  }
+}
+
+// After the FP64 residual R = B - A64 X: |r_c|, |R|_F and the stop test.
+// `init` (warm start) seeds the state without a stop test.
+__global__ void __launch_bounds__(kMT)
+    mp_after_residual_kernel(const double* __restrict__ R, int64_t n, int k, int init, double* bp,
+                             MpcgState* st, MpcgCols cols) {
+  if (st->done || (!init && !st->need_update)) return;
+  __shared__ double s_red[2 * (kMT / 32)];
+  const int c = blockIdx.y * kCW + threadIdx.x % kCW;
+  double acc = 0.0;
+  if (c < k) {
+    for (int64_t i = (int64_t)blockIdx.x * kRW + threadIdx.x / kCW; i < n;
+         i += (int64_t)gridDim.x * kRW) {
+      const double r = R[i * k + c];
+      acc = fma(r, r, acc);
+    }
+  }
+  const double v[1] = {acc};
+  store_col_partials<1>(v, bp, 0, k);
+  if (!arrive_last_block(&st->counters[kMCtrResid])) return;
+  const double tol = st->tol;
+  const bool freeze = st->column_stop && !init;
+  double fro = 0.0, live = 0.0;
+  bool nonfinite = false;
+  for (int cc = threadIdx.x; cc < k; cc += kMT) {
+    const double t = col_total(bp, gridDim.x, k, cc);
+    const double rn = sqrt(t);
+    cols.rn[cc] = rn;
+    fro += t;
+    if (!isfinite(rn)) nonfinite = true;
+    if (freeze && cols.live[cc] && rn <= tol * cols.bnorm[cc]) cols.live[cc] = 0;
+    live += cols.live[cc] ? 1.0 : 0.0;
+  }
+  double f[2] = {fro, live};
+  block_sum<kMT, 2>(f, s_red);
+  const int nf = __syncthreads_or(nonfinite ? 1 : 0);
+  if (threadIdx.x == 0) {
+    const double rn = sqrt(f[0]);
+    st->rnorm = rn;
+    st->true_rnorm = rn;
+    st->rmax = rn;
+    st->n_accurate += 1;
+    st->need_update = 0;
+    st->n_live = (int)f[1];
+    if (nf) {
+      mp_stop(st, LAKER_ERR_NONFINITE);
+    } else if (!init && (st->column_stop ? st->n_live == 0 : rn <= st->tol_abs)) {
+      mp_stop(st, LAKER_OK);
+    } else if (!init && st->iter >= st->max_iter) {
+      mp_stop(st, LAKER_ERR_NOT_CONVERGED);
+    }
+  }
+}
+
+// r_c . z_c -> beta_c (or rz_c seeded when `init`).  IDENT: the identity
+// preconditioner, Z = R rounded to FP32, written here.
+template <bool IDENT>
+__global__ void __launch_bounds__(kMT)
+    mp_after_precond_kernel(const double* __restrict__ R, float* __restrict__ Z, int64_t n, int k,
+                            int init, double* bp, MpcgState* st, MpcgCols cols) {
+  if (st->done) return;
+  const int c = blockIdx.y * kCW + threadIdx.x % kCW;
+  double acc = 0.0;
+  if (c < k) {
+    for (int64_t i = (int64_t)blockIdx.x * kRW + threadIdx.x / kCW; i < n;
+         i += (int64_t)gridDim.x * kRW) {
+      const int64_t e = i * k + c;
+      const double r = R[e];
+      float z;
+      if (IDENT) {
+        z = (float)r;
+        Z[e] = z;
+      } else {
+        z = Z[e];
+      }
+      acc = fma(r, (double)z, acc);
+    }
+  }
+  const double v[1] = {acc};
+  store_col_partials<1>(v, bp, 0, k);
+  if (!arrive_last_block(&st->counters[kMCtrPrecond])) return;
+  bool nonfinite = false;
+  for (int cc = threadIdx.x; cc < k; cc += kMT) {
+    const double t = col_total(bp, gridDim.x, k, cc);
+    if (!isfinite(t)) nonfinite = true;
+    if (init) {
+      cols.beta[cc] = 0.0;
+    } else {
+      const double rz = cols.rz[cc];
+      cols.beta[cc] = (cols.live[cc] && rz != 0.0) ? t / rz : 0.0;
+    }
+    cols.rz[cc] = t;
+  }
+  const int nf = __syncthreads_or(nonfinite ? 1 : 0);
+  if (threadIdx.x == 0 && nf) mp_stop(st, LAKER_ERR_NONFINITE);
+}
+
+// P = Z + P diag(beta) (P = Z when `init`); frozen columns get P_c = 0.
+__global__ void __launch_bounds__(kMT)
+    mp_update_p_kernel(const float* __restrict__ Z, float* __restrict__ P, int64_t n, int k,
+                       const MpcgState* st, MpcgCols cols, int init) {
+  if (st->done) return;
+  const int c = blockIdx.y * kCW + threadIdx.x % kCW;
+  if (c >= k) return;
+  const bool live = cols.live[c] != 0;
+  const float beta = (float)cols.beta[c];
+  for (int64_t i = (int64_t)blockIdx.x * kRW + threadIdx.x / kCW; i < n;
+       i += (int64_t)gridDim.x * kRW) {
+    const int64_t e = i * k + c;
+    P[e] = !live ? 0.0f : (init ? Z[e] : fmaf(beta, P[e], Z[e]));
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Multi-RHS factored CCCP apply Z = c^-1/2 R + Q (W (Q^T R)), three tiled
+// CUDA-core GEMMs (64 x 64 output tiles, 4 x 4 register microtiles):
+//   project  U_chunk = Q[rows of the chunk]^T R[rows of the chunk]  (FP32
+//            products summed in FP32 within a row chunk, stored as FP64)
+//   core     V = W U with U = sum of the chunks in chunk order     (FP64)
+//   expand   Z = c^-1/2 R + Q V                                      (FP32 sum)
+// It is only a preconditioner: FP32 sums change the iteration count, not the
+// accuracy of the solution, whose stop test is on the FP64 residual.  The
+// kernels read the first nq = round_up(N_r, 4) columns of Q (the columns from
+// N_r on are zero in the factor layout); ldq is Q's row stride.
+// ---------------------------------------------------------------------------
+namespace {
+
+__global__ void __launch_bounds__(kMT)
+    pcm_project_kernel(const float* __restrict__ Q, int ldq, int nq, const double* __restrict__ R,
+                       int64_t n, int k, int64_t chunk_rows, double* __restrict__ upart,
+                       const int* gate) {
+  if (gate && *gate == 0) return;
+  __shared__ __align__(16) float Qs[kGK][kGT];
+  __shared__ __align__(16) float Rs[kGK][kGT];
+  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+  const int j0 = blockIdx.x * kGT, c0 = blockIdx.y * kGT;
+  const int64_t i_begin = (int64_t)blockIdx.z * chunk_rows;
+  const int64_t i_end = min(n, i_begin + chunk_rows);
+  float acc[4][4] = {};
+  const int rr = tid / 16, cg = tid % 16;
+  for (int64_t i = i_begin; i < i_end; i += kGK) {
+    const int64_t ii = i + rr;
+    const bool row_ok = ii < i_end;
+    {
+      const int j = j0 + cg * 4;
+      float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (row_ok && j < nq) q = *reinterpret_cast<const float4*>(Q + ii * ldq + j);
+      *reinterpret_cast<float4*>(&Qs[rr][cg * 4]) = q;
+    }
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int c = c0 + cg * 4 + v;
+      Rs[rr][cg * 4 + v] = (row_ok && c < k) ? (float)R[ii * k + c] : 0.0f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kGK; ++kk) {
+      const float4 a = *reinterpret_cast<const float4*>(&Qs[kk][ty * 4]);
+      const float4 b = *reinterpret_cast<const float4*>(&Rs[kk][tx * 4]);
+      const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(av[u], bv[v], acc[u][v]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int j = j0 + ty * 4 + u;
+    if (j >= nq) continue;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int c = c0 + tx * 4 + v;
+      if (c < k) upart[((int64_t)blockIdx.z * nq + j) * k + c] = (double)acc[u][v];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kMT)
+    pcm_core_kernel(const float* __restrict__ W, int nr, int nq, const double* __restrict__ upart,
+                    int nchunk, int k, double* __restrict__ V, const int* gate) {
+  if (gate && *gate == 0) return;
+  __shared__ double Ws[kGK][kGT];
+  __shared__ double Us[kGK][kGT];
+  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+  const int j0 = blockIdx.x * kGT, c0 = blockIdx.y * kGT;
+  const int rr = tid / 16, cg = tid % 16;
+  double acc[4][4] = {};
+  for (int jp = 0; jp < nr; jp += kGK) {
+    const int jj = jp + rr;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int j = j0 + cg * 4 + v;
+      // W is symmetric: W[j][jj] = W[jj][j] (row jj read contiguously)
+      Ws[rr][cg * 4 + v] = (jj < nr && j < nr) ? (double)W[(int64_t)jj * nr + j] : 0.0;
+      const int c = c0 + cg * 4 + v;
+      double u = 0.0;
+      if (jj < nr && c < k)
+        for (int ch = 0; ch < nchunk; ++ch) u += upart[((int64_t)ch * nq + jj) * k + c];
+      Us[rr][cg * 4 + v] = u;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kGK; ++kk) {
+      double av[4], bv[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) av[u] = Ws[kk][ty * 4 + u], bv[u] = Us[kk][tx * 4 + u];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = fma(av[u], bv[v], acc[u][v]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int j = j0 + ty * 4 + u;
+    if (j >= nq) continue;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int c = c0 + tx * 4 + v;
+      if (c < k) V[(int64_t)j * k + c] = acc[u][v];
+    }
+  }
+}
+
+template <typename ZT>
+__global__ void __launch_bounds__(kMT)
+    pcm_expand_kernel(const float* __restrict__ Q, int ldq, int nq, int nr,
+                      const double* __restrict__ V, const double* __restrict__ R, double cis,
+                      int64_t n, int k, ZT* __restrict__ Z, const int* gate) {
+  if (gate && *gate == 0) return;
+  __shared__ __align__(16) float Qs[kGK][kGT + 4];  // transposed: Qs[j][i]
+  __shared__ __align__(16) float Vs[kGK][kGT];
+  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+  const int64_t i0 = (int64_t)blockIdx.x * kGT;
+  const int c0 = blockIdx.y * kGT;
+  float acc[4][4] = {};
+  for (int j = 0; j < nr; j += kGK) {
+    {
+      const int ii = tid / 4, cg = tid % 4;  // 64 rows x 4 groups of 4 columns
+      const int64_t i = i0 + ii;
+      const int jc = j + cg * 4;
+      float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (i < n && jc < nq) q = *reinterpret_cast<const float4*>(Q + i * ldq + jc);
+      Qs[cg * 4 + 0][ii] = q.x;
+      Qs[cg * 4 + 1][ii] = q.y;
+      Qs[cg * 4 + 2][ii] = q.z;
+      Qs[cg * 4 + 3][ii] = q.w;
+    }
+    {
+      const int rr = tid / 16, cg = tid % 16;
+      const int jr = j + rr;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int c = c0 + cg * 4 + v;
+        Vs[rr][cg * 4 + v] = (jr < nr && c < k) ? (float)V[(int64_t)jr * k + c] : 0.0f;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kGK; ++kk) {
+      const float4 a = *reinterpret_cast<const float4*>(&Qs[kk][ty * 4]);
+      const float4 b = *reinterpret_cast<const float4*>(&Vs[kk][tx * 4]);
+      const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(av[u], bv[v], acc[u][v]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int64_t i = i0 + ty * 4 + u;
+    if (i >= n) continue;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int c = c0 + tx * 4 + v;
+      if (c < k) {
+        const int64_t e = i * k + c;
+        Z[e] = (ZT)(cis * R[e] + (double)acc[u][v]);
+      }
+    }
+  }
+}
+
+// Columns of Q the apply reads: N_r rounded up to a float4.
+int pcm_cols(int nr) { return (int)round_up(nr, 4); }
+
+int pcm_tiles(int nq, int k) { return (int)(ceil_div(nq, kGT) * ceil_div(k, kGT)); }
+
+int pcm_chunks(int64_t n, int nq, int k) {
+  int64_t c = ceil_div(2 * (int64_t)sm_count(), pcm_tiles(nq, k));
+  const int64_t lim = ceil_div(n, 256);
+  if (c > lim) c = lim;
+  if (c > 64) c = 64;
+  return (int)(c < 1 ? 1 : c);
+}
+
+}  // namespace
+
+size_t precond_multi_scratch_bytes(int64_t n, int nr, int k) {
+  const int nq = pcm_cols(nr);
+  const int nch = pcm_chunks(n, nq, k);
+  return (size_t)round_up((int64_t)((size_t)nch * nq * k * sizeof(double)), 256) +
+         (size_t)round_up((int64_t)((size_t)nq * k * sizeof(double)), 256);
+}
+
+template <typename ZT>
+cudaError_t launch_precond_multi(const laker_precond* pc, const double* R, int k, ZT* Z,
+                                 void* scratch, const int* gate, cudaStream_t s) {
+  const int64_t n = pc->n;
+  const int ldq = pc->ldq, nr = pc->nr, nq = pcm_cols(nr);
+  const int nch = pcm_chunks(n, nq, k);
+  double* upart = static_cast<double*>(scratch);
+  double* V = reinterpret_cast<double*>(static_cast<char*>(scratch) +
+                                        round_up((int64_t)((size_t)nch * nq * k * sizeof(double)), 256));
+  const int64_t chunk_rows = round_up(ceil_div(n, nch), kGK);
+  const unsigned gy = (unsigned)ceil_div(k, kGT);
+  pcm_project_kernel<<<dim3((unsigned)ceil_div(nq, kGT), gy, (unsigned)nch), kMT, 0, s>>>(
+      pc->q_basis, ldq, nq, R, n, k, chunk_rows, upart, gate);
+  pcm_core_kernel<<<dim3((unsigned)ceil_div(nq, kGT), gy), kMT, 0, s>>>(pc->w_core, nr, nq, upart,
+                                                                      nch, k, V, gate);
+  pcm_expand_kernel<ZT><<<dim3((unsigned)ceil_div(n, kGT), gy), kMT, 0, s>>>(
+      pc->q_basis, ldq, nq, nr, V, R, pc->inv_sqrt_iso, n, k, Z, gate);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_precond_multi<float>(const laker_precond*, const double*, int, float*,
+                                                 void*, const int*, cudaStream_t);
+template cudaError_t launch_precond_multi<double>(const laker_precond*, const double*, int, double*,
+                                                  void*, const int*, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// The multi-RHS solve.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct MpcgWs {
+  WsHeader* hdr;
+  MpcgState* st;
+  MpcgCols cols;
+  double* R;
+  float* P;
+  float* AP;
+  float* Z;
+  double* bp;
+  void* pscratch;
+  uint8_t* img;
+  size_t bytes;
+};
+
+// Graph of one iteration (released when the solve returns).
+struct MpcgGraph {
+  cudaStream_t cap = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  ~MpcgGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (cap) cudaStreamDestroy(cap);
+  }
+};
+
+MpcgWs carve_multi(void* base, int64_t n, int k, int nr) {
+  MpcgWs w{};
+  char* p = static_cast<char*>(base);
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    char* q = p ? p + off : nullptr;
+    off += (size_t)round_up((int64_t)bytes, 256);
+    return q;
+  };
+  const size_t nk = (size_t)n * (size_t)k;
+  const ColGrid g = col_grid(n, k);
+  w.hdr = reinterpret_cast<WsHeader*>(take(kWsHeader));
+  w.st = reinterpret_cast<MpcgState*>(take(sizeof(MpcgState)));
+  w.cols.bnorm = reinterpret_cast<double*>(take((size_t)k * sizeof(double)));
+  w.cols.rz = reinterpret_cast<double*>(take((size_t)k * sizeof(double)));
+  w.cols.alpha = reinterpret_cast<double*>(take((size_t)k * sizeof(double)));
+  w.cols.beta = reinterpret_cast<double*>(take((size_t)k * sizeof(double)));
+  w.cols.rn = reinterpret_cast<double*>(take((size_t)k * sizeof(double)));
+  w.cols.live = reinterpret_cast<int*>(take((size_t)k * sizeof(int)));
+  w.R = reinterpret_cast<double*>(take(nk * sizeof(double)));
+  w.P = reinterpret_cast<float*>(take(nk * sizeof(float)));
+  w.AP = reinterpret_cast<float*>(take(nk * sizeof(float)));
+  w.Z = reinterpret_cast<float*>(take(nk * sizeof(float)));
+  w.bp = reinterpret_cast<double*>(take((size_t)3 * g.gx * (size_t)k * sizeof(double)));
+  w.pscratch = nr > 0 ? take(precond_multi_scratch_bytes(n, nr, k)) : nullptr;
+  w.img = k2_use_tensor_cores() ? reinterpret_cast<uint8_t*>(take(k2_image_bytes(n, n, k))) : nullptr;
+  w.bytes = off;
+  return w;
+}
+
+}  // namespace
+
+size_t pcg_multi_workspace_bytes(int64_t n, int d, int nr, int k) {
+  (void)d;
+  return carve_multi(nullptr, n, k, nr).bytes;
+}
+
+int pcg_solve_multi(const laker_operator* op, const laker_precond* pc, const double* B, int k,
+                    double* X, const laker_pcg_params* prm, void* workspace, laker_pcg_result* res,
+                    cudaStream_t s) {
+  const int64_t n = op->n;
+  const int d = op->d;
+  const int nr = pc ? pc->nr : 0;
+  MpcgWs w = carve_multi(workspace, n, k, nr);
+  const ColGrid g = col_grid(n, k);
+  const dim3 cgrid((unsigned)g.gx, (unsigned)g.gy);
+  int* dstatus = &w.hdr->status;
+  const float lam32 = (float)op->lambda_reg;
+
+  *res = laker_pcg_result{};
+  MpcgState h{};
+  h.tol = prm->tol;
+  h.delta = prm->reliable_delta;
+  h.eps = prm->breakdown_eps;
+  h.max_iter = prm->max_iter;
+  h.active = 1;
+  h.column_stop = prm->column_stop ? 1 : 0;
+  cudaError_t e = cudaMemsetAsync(w.hdr, 0, kWsHeader, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(w.st, &h, sizeof(MpcgState), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return fail_cuda(e);
+
+  int launches = 0;
+  // R = B - A64 X (gated by `gate`; ungated for the warm start)
+  auto launch_residual = [&](int init, const int* gate, cudaStream_t cs) -> cudaError_t {
+    cudaError_t ee = launch_multi_f64(op->packed64, n, op->packed64, n, d, op->lambda_reg, op->clamp,
+                                      X, k, k, B, k, w.R, k, cs, gate);
+    if (ee == cudaSuccess)
+      mp_after_residual_kernel<<<cgrid, kMT, 0, cs>>>(w.R, n, k, init, w.bp, w.st, w.cols);
+    launches += 2;
+    return ee;
+  };
+  auto launch_precond = [&](int init, cudaStream_t cs) -> cudaError_t {
+    cudaError_t ee = cudaSuccess;
+    if (pc) {
+      ee = launch_precond_multi<float>(pc, w.R, k, w.Z, w.pscratch, &w.st->active, cs);
+      mp_after_precond_kernel<false><<<cgrid, kMT, 0, cs>>>(w.R, w.Z, n, k, init, w.bp, w.st, w.cols);
+      launches += 4;
+    } else {
+      mp_after_precond_kernel<true><<<cgrid, kMT, 0, cs>>>(w.R, w.Z, n, k, init, w.bp, w.st, w.cols);
+      launches += 1;
+    }
+    mp_update_p_kernel<<<cgrid, kMT, 0, cs>>>(w.Z, w.P, n, k, w.st, w.cols, init);
+    launches += 1;
+    return ee;
+  };
+
+  // ---- initialisation ------------------------------------------------------
+  mp_init_kernel<<<cgrid, kMT, 0, s>>>(B, X, w.R, n, k, prm->has_x0, w.bp, w.st, w.cols);
+  launches += 1;
+  e = cudaGetLastError();
+  if (e == cudaSuccess && prm->has_x0) e = launch_residual(1, nullptr, s);
+  if (e != cudaSuccess) return fail_cuda(e);
+  e = cudaMemcpyAsync(&h, w.st, sizeof(MpcgState), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fail_cuda(e);
+  res->rhs_norm = h.bnorm;
+  res->kernel_launches = launches;
+  if (h.bnorm == 0.0) {
+    // zero right-hand side: X is returned unchanged (zero, or the warm start)
+    res->status = LAKER_OK;
+    res->residual_norm = 0.0;
+    return LAKER_OK;
+  }
+  if (h.done) {
+    res->status = h.status;
+    res->residual_norm = h.true_rnorm;
+    return h.status;
+  }
+  e = launch_precond(1, s);
+  if (e != cudaSuccess) return fail_cuda(e);
+
+  // ---- iterations ------------------------------------------------------------
+  auto iteration = [&](cudaStream_t cs) -> cudaError_t {
+    cudaError_t ee;
+    if (w.img)
+      ee = launch_k2(op->packed32, n, op->packed32, n, d, op->clamp, lam32, w.P, k, k, w.AP, k, w.img,
+                     dstatus, cs, &w.st->active);
+    else
+      ee = launch_multi_f32(op->packed32, n, op->packed32, n, d, lam32, op->clamp, w.P, k, k, w.AP, k,
+                            cs, &w.st->active);
+    launches += w.img ? 3 : 1;
+    if (ee != cudaSuccess) return ee;
+    mp_after_matvec_kernel<<<cgrid, kMT, 0, cs>>>(w.P, w.AP, n, k, w.bp, w.st, w.cols, dstatus);
+    mp_update_xr_kernel<<<cgrid, kMT, 0, cs>>>(w.P, w.AP, X, w.R, n, k, w.bp, w.st, w.cols);
+    launches += 2;
+    ee = launch_residual(0, &w.st->need_update, cs);
+    if (ee != cudaSuccess) return ee;
+    return launch_precond(0, cs);
+  };
+  MpcgGraph ig;
+  int iter_launches = 0;
+  {
+    const int before = launches;
+    e = cudaStreamCreateWithFlags(&ig.cap, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamBeginCapture(ig.cap, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      const cudaError_t ie = iteration(ig.cap);
+      const cudaError_t ce = cudaGetLastError();
+      e = cudaStreamEndCapture(ig.cap, &ig.graph);
+      if (e == cudaSuccess) e = ie != cudaSuccess ? ie : ce;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&ig.exec, ig.graph, 0);
+    if (e != cudaSuccess) return fail_cuda(e);
+    iter_launches = launches - before;
+    launches = before;
+  }
+  // Polls: the first after one iteration, whose host-measured time sets the
+  // replays between later polls (about 10 ms of work, at most 64).
+  int check = prm->check_every > 0 ? prm->check_every : 1;
+  bool calibrate = prm->check_every <= 0;
+  int launched = 0;
+  while (launched < prm->max_iter) {
+    const int chunk = (prm->max_iter - launched) < check ? (prm->max_iter - launched) : check;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int c = 0; c < chunk; ++c) {
+      e = cudaGraphLaunch(ig.exec, s);
+      if (e != cudaSuccess) return fail_cuda(e);
+      launches += iter_launches;
+    }
+    launched += chunk;
+    e = cudaMemcpyAsync(&h, w.st, sizeof(MpcgState), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail_cuda(e);
+    if (h.done) break;
+    if (calibrate) {
+      const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      const double per = dt / chunk;
+      check = per > 0.0 ? (int)(0.01 / per) : 64;
+      if (check < 1) check = 1;
+      if (check > 64) check = 64;
+      calibrate = false;
+    }
+  }
+
+  int dev_status = 0;
+  e = cudaMemcpyAsync(&dev_status, dstatus, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fail_cuda(e);
+  res->iterations = h.iter;
+  res->accurate_matvecs = h.n_accurate;
+  res->residual_norm = h.true_rnorm;
+  res->recurrence_norm = h.rnorm;
+  res->rhs_norm = h.bnorm;
+  res->kernel_launches = launches;
+  if (dev_status != 0) {
+    res->status = dev_status;
+    return dev_status;
+  }
+  if (!h.done) {
+    res->status = LAKER_ERR_NOT_CONVERGED;
+    return LAKER_ERR_NOT_CONVERGED;
+  }
+  res->status = h.status;
+  return h.status;
+}
+
+}  // namespace laker

@@ -26,6 +26,7 @@ using namespace laker;
 
 extern "C" size_t laker_precond_workspace_bytes(int64_t n, int nr, int k) {
   if (n < 0 || nr < 1 || nr > kMaxNr || k < 1) return 0;
+  if (k > 1) return kWsHeader + precond_multi_scratch_bytes(n, nr, k);
   const size_t G = (size_t)precond_grid();
   // header | counters | upart (G x 1024) | v (1024) | blockpart (G)
   return kWsHeader + 256 + round_up((int64_t)(G * kMaxNr * sizeof(double)), 256) +
@@ -39,9 +40,18 @@ extern "C" int laker_precond_apply(const laker_precond* pc, const double* R, int
   if (!pc || k < 1 || ldr < k || ldz < k) return LAKER_ERR_INVALID_ARG;
   if (pc->n == 0 && pc->nr >= 1) return LAKER_OK;
   if (!precond_valid(pc) || !R || !Z || !workspace) return LAKER_ERR_INVALID_ARG;
-  if (k != 1 || ldr != 1 || ldz != 1) return LAKER_ERR_UNSUPPORTED;
   if (workspace_bytes < laker_precond_workspace_bytes(pc->n, pc->nr, k)) return LAKER_ERR_WORKSPACE;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (k > 1) {
+    // k right-hand sides: three tiled GEMMs over (n x k) row-major R and Z
+    if (ldr != k || ldz != k) return LAKER_ERR_UNSUPPORTED;
+    void* scratch = static_cast<char*>(workspace) + kWsHeader;
+    const cudaError_t e = z_is_f64
+        ? launch_precond_multi<double>(pc, R, k, static_cast<double*>(Z), scratch, nullptr, s)
+        : launch_precond_multi<float>(pc, R, k, static_cast<float*>(Z), scratch, nullptr, s);
+    return e == cudaSuccess ? LAKER_OK : fail_cuda(e);
+  }
+  if (ldr != 1 || ldz != 1) return LAKER_ERR_UNSUPPORTED;
   const int G = precond_grid();
   char* base = static_cast<char*>(workspace);
   WsHeader* hdr = reinterpret_cast<WsHeader*>(base);

@@ -155,9 +155,11 @@ cudaError_t launch_k1t_batched(const uint8_t* img, int clamp, const float* x, do
                                float* colpart, const SymPlan& sp, const BatchMap& bm, int* status,
                                const int* gate, cudaStream_t s, int fmt = kK1tTf32);
 // y = lam x + (sum of the partials) for the standalone matvec.
+// Outputs are NaN when *status reports a failure of the kernel that wrote the
+// partials (status may be null).
 cudaError_t launch_sym_finish(const SymPlan& sp, const double* rowpart, const float* colpart,
                               int64_t n, float lam, const float* x, float* y, int64_t ldy,
-                              cudaStream_t s);
+                              const int* status, cudaStream_t s);
 // Whether square FP32 matvecs use the symmetric kernel (LAKER_K1_SYMMETRIC=0
 // selects the plain one, for comparisons).
 bool k1_use_symmetric();
@@ -189,7 +191,8 @@ cudaError_t launch_k4s_batched(const double* E64, int d, int clamp, const double
 // y = [b -] (lam x + K64 x) from the FP64 partials (b may be null).
 cudaError_t launch_sym_finish64(const SymPlan& sp, const double* rowpart, const double* colpart,
                                 int64_t n, double lam, const double* x, const double* b,
-                                int64_t ldb, double* y, int64_t ldy, cudaStream_t s);
+                                int64_t ldb, double* y, int64_t ldy, const int* status,
+                                cudaStream_t s);
 // Whether the FP64 residual uses the symmetric kernel (LAKER_K4_SYMMETRIC=0
 // selects the plain one).
 bool k4_use_symmetric();

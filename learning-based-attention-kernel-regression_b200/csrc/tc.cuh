@@ -146,17 +146,24 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// Wait for a phase, giving up on timeout (~2 s; sets *abort and records
-// LAKER_ERR_TIMEOUT) or when another role has set *abort.
+// Wait for a phase, giving up on timeout (the wait limit, ~2 s by default, or
+// at once for a limit of 0; sets *abort and records LAKER_ERR_TIMEOUT) or
+// when another role has set *abort.
 __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, int* status,
                                               volatile int* abort) {
+  const unsigned long long limit = wait_limit_ns();
+  if (limit == 0) {
+    record_status(status, LAKER_ERR_TIMEOUT);
+    *abort = 1;
+    return false;
+  }
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_timer_ns();
   for (uint32_t it = 0; it < (1u << 30); ++it) {
     if (mbar_try_wait(bar, parity)) return true;
     if ((it & 63u) == 0) {
       if (*abort) return false;
-      if (global_timer_ns() - t0 > 2000000000ull) break;
+      if (global_timer_ns() - t0 >= limit) break;
     }
   }
   record_status(status, LAKER_ERR_TIMEOUT);

@@ -10,8 +10,11 @@
 namespace laker {
 namespace {
 
-constexpr int kNumVariants = 6;
-std::atomic<int> g_variant[kNumVariants] = {{-1}, {-1}, {-1}, {-1}, {-1}, {-1}};
+constexpr int kNumVariants = 7;
+std::atomic<int> g_variant[kNumVariants] = {{-1}, {-1}, {-1}, {-1}, {-1}, {-1}, {-1}};
+
+// Default bounded-wait limit: 2 s.
+constexpr int kWaitLimitDefaultUs = 2000000;
 
 int variant_default(int which) {
   if (which == LAKER_VARIANT_K1T_UNIT) {
@@ -36,6 +39,7 @@ int variant_default(int which) {
     const char* e = getenv("LAKER_K1T_F16");
     return (e && e[0] == '0') ? 0 : 1;
   }
+  if (which == LAKER_VARIANT_WAIT_LIMIT_US) return kWaitLimitDefaultUs;
   const char* e = getenv("LAKER_K2_LOGITS_TC");
   return (e && e[0] == '1') ? 1 : 0;
 }
@@ -44,7 +48,22 @@ bool variant_valid(int which, int value) {
   if (which == LAKER_VARIANT_K1T_UNIT) return value == 2 || value == 4;
   if (which == LAKER_VARIANT_SYM_MIN_BLOCKS) return value >= 0 && value <= 64;
   if (which == LAKER_VARIANT_K1T_LOGITS) return value == 0 || value == 1;
+  if (which == LAKER_VARIANT_WAIT_LIMIT_US) return value >= 0 && value <= kWaitLimitDefaultUs;
   return value == 0 || value == 1;
+}
+
+// Writes the wait limit into every translation unit's copy on the current
+// device.
+cudaError_t apply_wait_limit(int us) {
+  const unsigned long long ns = (unsigned long long)us * 1000ull;
+  cudaError_t (*const setters[])(unsigned long long) = {set_wait_limit_f32, set_wait_limit_f64,
+                                                        set_wait_limit_sym, set_wait_limit_symtc,
+                                                        set_wait_limit_tc};
+  for (auto f : setters) {
+    const cudaError_t e = f(ns);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace
@@ -67,6 +86,13 @@ using namespace laker;
 extern "C" int laker_set_variant(int which, int value) {
   if (which < 0 || which >= kNumVariants || !variant_valid(which, value)) return -1;
   const int prev = variant_get(which);
+  if (which == LAKER_VARIANT_WAIT_LIMIT_US) {
+    const cudaError_t e = apply_wait_limit(value);
+    if (e != cudaSuccess) {
+      fail_cuda(e);
+      return -1;
+    }
+  }
   g_variant[which].store(value, std::memory_order_relaxed);
   return prev;
 }

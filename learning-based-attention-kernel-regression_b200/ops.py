@@ -122,11 +122,14 @@ def pcg_solve(packed32: torch.Tensor, packed64: torch.Tensor, n: int, d: int, la
               clamp: bool, q32: Optional[torch.Tensor], w32: Optional[torch.Tensor], nr: int,
               inv_sqrt_iso: float, b: torch.Tensor, x0: Optional[torch.Tensor], tol: float,
               max_iter: int, reliable_delta: float, breakdown_eps: float, check_every: int,
-              profile: bool) -> Tuple[torch.Tensor, torch.Tensor]:
-    """Fused mixed-precision PCG for one right-hand side b (n,): returns x
-    (FP64) and the solve's report as a float64 CPU tensor in the order of
-    STATS_FIELDS (status, iterations, ...).  A breakdown, non-finite value or
-    the iteration cap is reported in the status, not raised."""
+              profile: bool, column_stop: bool = False) -> Tuple[torch.Tensor, torch.Tensor]:
+    """Fused mixed-precision PCG for b of shape (n,) or (n, k): returns x
+    (FP64, b's shape) and the solve's report as a float64 CPU tensor in the
+    order of STATS_FIELDS (status, iterations, ...).  For k right-hand sides
+    alpha and beta are per column and the stop test is the Frobenius one of
+    the reference's solve_2d, or per column with `column_stop`.  A breakdown,
+    non-finite value or the iteration cap is reported in the status, not
+    raised."""
     op = _lib.laker_operator(packed32.data_ptr(), packed64.data_ptr(), n, d, float(lam), int(clamp))
     pc = _lib.precond_struct(q32, w32, n, nr, inv_sqrt_iso) if q32 is not None else None
     bb = b.to(torch.float64).contiguous()
@@ -134,7 +137,7 @@ def pcg_solve(packed32: torch.Tensor, packed64: torch.Tensor, n: int, d: int, la
         else torch.empty_like(bb)
     params = _lib.laker_pcg_params(float(tol), int(max_iter), float(reliable_delta),
                                    float(breakdown_eps), int(check_every), int(x0 is not None),
-                                   int(profile))
+                                   int(profile), int(column_stop))
     res = _lib.pcg_solve(op, pc, bb, x, params)
     stats = torch.tensor([float(getattr(res, f)) for f in STATS_FIELDS], dtype=torch.float64)
     return x, stats
@@ -142,7 +145,8 @@ def pcg_solve(packed32: torch.Tensor, packed64: torch.Tensor, n: int, d: int, la
 
 @pcg_solve.register_fake
 def _pcg_solve_fake(packed32, packed64, n, d, lam, clamp, q32, w32, nr, inv_sqrt_iso, b, x0, tol,
-                    max_iter, reliable_delta, breakdown_eps, check_every, profile):
+                    max_iter, reliable_delta, breakdown_eps, check_every, profile,
+                    column_stop=False):
     return (b.new_empty(b.shape, dtype=torch.float64),
             torch.empty(len(STATS_FIELDS), dtype=torch.float64, device="cpu"))
 

@@ -202,6 +202,7 @@ class CCCPPreconditioner:
         # operator(probes) through the fused multi-RHS kernel; QR and the
         # N_r x N_r fixed point then run in float64 on the GPU
         op_probes = operator(probes).to(torch.float64)
+        _lib.raise_device_status(dev)
         clock.stop("operator")
         dt = torch.float64
         norms = torch.linalg.norm(op_probes, dim=0, keepdim=True)
@@ -364,10 +365,10 @@ class CCCPPreconditioner:
 
     def apply_2d(self, x: torch.Tensor) -> torch.Tensor:
         _lib.require_cuda(x, "x")
-        # k right-hand sides: three plain GEMMs (cuBLAS) with the same folded W
-        q = self._q32[:, : self.nr].to(x.dtype)
-        w = self._w32.to(x.dtype)
-        return (self.isotropic_coef ** (-0.5)) * x + q @ (w @ (q.T @ x))
+        # k right-hand sides: the multi-RHS fused apply (the one the device
+        # multi-RHS solve uses), with the same folded factors
+        q32, w32, nr, cis = self.apply_factors()
+        return ops.precond_apply(q32, w32, self.n, nr, cis, x, x.dtype == torch.float64)
 
     def apply_impl(self, x: torch.Tensor) -> torch.Tensor:
         return self.apply(x)

@@ -7,15 +7,17 @@ attributes, ValueError for a rhs that is not 1-D or 2-D, RuntimeError on
 breakdown, zero RHS returned as is, and a warning when max_iter is reached.
 
 When `operator` is the bound `matvec` of an AttentionKernelOperator and
-`preconditioner` the bound `apply` of a CCCPPreconditioner (or None), a 1-D
+`preconditioner` the bound `apply` of a CCCPPreconditioner (or None), the
 solve runs entirely on the device through laker_pcg_solve: FP32 fused
 operator inside the recurrence, FP64 vectors / inner products / scalars, and
 reliable updates that replace the recurrence residual by the FP64 residual
 b - A x, so the stop test `||b - A x|| <= tol ||b||` holds for the float64
-operator.  2-D right-hand sides with the attention operator use the same
-mixed-precision recurrence (column-wise alpha/beta, global Frobenius stop
-test as in solve_2d) driven from torch with the fused multi-RHS kernels.  Any
-other callables run the reference recurrence unchanged on their CUDA tensors.
+operator.  2-D right-hand sides take the same device loop with column-wise
+alpha / beta and the global Frobenius stop test of solve_2d (or, with
+`column_stop=True`, a per-column stop).  With a row-sharded operator 2-D
+right-hand sides run the same mixed-precision recurrence driven from torch
+over the sharded products.  Any other callables run the reference recurrence
+unchanged on their CUDA tensors.
 """
 
 from __future__ import annotations
@@ -55,6 +57,9 @@ class PreconditionedConjugateGradient:
             recurrence residual fell by this factor since the last
             recomputation (mixed-precision reliable update).
         check_every: host polls of the device status (0 = automatic).
+        column_stop: 2-D right-hand sides only: stop each column on its own
+            FP64 residual (||b_c - A x_c|| <= tol ||b_c||, the column is then
+            frozen) instead of the reference's global Frobenius test.
 
     Extra attributes after solve: `accurate_matvecs` (FP64 residual
     recomputations), `recurrence_norm`, `status` (laker status code).
@@ -71,6 +76,7 @@ class PreconditionedConjugateGradient:
         reliable_delta: float = 0.03,
         check_every: int = 0,
         profile: bool = False,
+        column_stop: bool = False,
     ) -> None:
         self.tol = float(tol)
         self.max_iter = max_iter
@@ -81,6 +87,7 @@ class PreconditionedConjugateGradient:
         self.reliable_delta = float(reliable_delta)
         self.check_every = int(check_every)
         self.profile = bool(profile)
+        self.column_stop = bool(column_stop)
         self.last_result: Optional[_lib.laker_pcg_result] = None
         self.iterations: int = 0
         self.residual_norm: float = float("inf")
@@ -112,20 +119,24 @@ class PreconditionedConjugateGradient:
             pc = _bound_self(preconditioner, CCCPPreconditioner, ("apply", "apply_1d", "apply_impl"))
             fused_pc = pc is not None
         if op is not None and fused_pc and not self.autograd_safe and self.restart_freq is None:
-            if rhs.dim() == 1 and isinstance(op, DistributedAttentionKernelOperator) \
-                    and not op.single_device:
-                return self._solve_sharded(op, pc, rhs, x0, max_iter)
-            if rhs.dim() == 1:
-                return self._solve_fused(op, pc, rhs, x0, max_iter)
-            return self._solve_mixed_2d(op, preconditioner, rhs, x0, max_iter)
+            if isinstance(op, DistributedAttentionKernelOperator) and not op.single_device:
+                if rhs.dim() == 1:
+                    return self._solve_sharded(op, pc, rhs, x0, max_iter)
+                return self._solve_mixed_2d(op, preconditioner, rhs, x0, max_iter)
+            return self._solve_fused(op, pc, rhs, x0, max_iter)
         if preconditioner is None:
             preconditioner = lambda v: v  # noqa: E731
-        return self._solve_generic(operator, preconditioner, rhs, x0, max_iter)
+        x = self._solve_generic(operator, preconditioner, rhs, x0, max_iter)
+        _lib.raise_device_status(rhs.device)
+        return x
 
     # ------------------------------------------------------------------
     def _finish(self, status: int, rel: float) -> None:
         if status == _lib.LAKER_ERR_BREAKDOWN:
             raise RuntimeError(BREAKDOWN_MSG)
+        if status == _lib.LAKER_ERR_TIMEOUT:
+            raise _lib.LakerError(status, "PCG", _lib.status_string(status) +
+                                  " (a bounded wait on the GPU expired; the solve was stopped)")
         if status == _lib.LAKER_ERR_NONFINITE:
             raise RuntimeError("PCG encountered a non-finite inner product (NaN/Inf in the data)")
         if status == _lib.LAKER_ERR_NOT_CONVERGED:
@@ -142,7 +153,7 @@ class PreconditionedConjugateGradient:
         x, stats = ops.pcg_solve(
             p.packed32, p.packed64, op.n, op.embedding_dim, op.lambda_reg, not op.skip_clamp,
             q32, w32, nr, cis, rhs, x0, self.tol, int(max_iter), self.reliable_delta,
-            self._eps(rhs.dtype), self.check_every, self.profile)
+            self._eps(rhs.dtype), self.check_every, self.profile, self.column_stop)
         res = ops.result_from_stats(stats)
         self.last_result = res
         self.iterations = int(res.iterations)
@@ -180,7 +191,9 @@ class PreconditionedConjugateGradient:
         return x.to(rhs.dtype)
 
     def _solve_mixed_2d(self, op: AttentionKernelOperator, preconditioner, rhs, x0, max_iter):
-        """Mixed-precision 2-D recurrence (solve_2d semantics, FP64 residual)."""
+        """Mixed-precision 2-D recurrence (solve_2d semantics, FP64 residual)
+        driven from torch, for the row-sharded operator whose products
+        exchange rows between ranks on the host side."""
         b = rhs.to(torch.float64)
         pre = preconditioner if preconditioner is not None else (lambda v: v)
         if x0 is None:
@@ -214,6 +227,7 @@ class PreconditionedConjugateGradient:
             x.add_(p * alpha.unsqueeze(0))
             r.sub_(ap * alpha.unsqueeze(0))
             rn = torch.linalg.norm(r).item()
+            _lib.raise_device_status(r.device)
             self.recurrence_norm = rn
             rmax = max(rmax, rn)  # running max since the last FP64 recomputation
             if rn <= self.reliable_delta * rmax or rn <= self.tol * bn or it == max_iter:

@@ -25,17 +25,32 @@ def rel(a, b):
     return float((a - b).norm() / b.norm())
 
 
+def _free_bytes_settled(cuda, expect):
+    """Device free memory, read again once if it differs (another context on
+    the GPU can change it between two reads)."""
+    free = torch.cuda.mem_get_info(cuda)[0]
+    if free != expect:
+        torch.cuda.synchronize()
+        free = torch.cuda.mem_get_info(cuda)[0]
+    return free
+
+
 def test_noalloc_matches_workspace_entry_point_twice(cuda):
+    """Two calls in a row, of different sizes (so the segment split of the
+    scratch differs between them), each against the workspace entry point
+    and the float64 oracle."""
     from laker_b200 import _lib
+    from oracle import laker_oracle as O
 
     lib = _lib.load()
     rng = np.random.default_rng(21)
-    n, d = 3001, 10
-    E = torch.tensor(rng.standard_normal((n, d)) * 0.5, device=cuda, dtype=torch.float32)
-    packed = _lib.pack_f32(E)
+    d = 10
     stream = _lib.stream_handle(cuda)
-    for call, lam in enumerate((0.01, 0.3)):
-        x = torch.tensor(rng.standard_normal(n), device=cuda, dtype=torch.float32)
+    for call, (n, lam) in enumerate(((3001, 0.01), (9000, 0.3))):
+        E_np = (rng.standard_normal((n, d)) * 0.5).astype(np.float32)
+        packed = _lib.pack_f32(torch.tensor(E_np, device=cuda))
+        x_np = rng.standard_normal(n).astype(np.float32)
+        x = torch.tensor(x_np, device=cuda)
         ref = _lib.attn_matvec_f32(packed, n, packed, n, d, lam, 0, x)
         y = torch.full((n,), float("nan"), device=cuda, dtype=torch.float32)
         torch.cuda.synchronize()
@@ -44,12 +59,14 @@ def test_noalloc_matches_workspace_entry_point_twice(cuda):
                                                ctypes.c_float(lam), 0, x.data_ptr(),
                                                y.data_ptr(), stream)
         assert st == _lib.LAKER_OK, _lib.status_string(st)
-        torch.cuda.synchronize()
+        assert _lib.noalloc_status(cuda) == _lib.LAKER_OK
         if call == 1:
             # after the first call set the scratch up, calls allocate nothing
-            assert torch.cuda.mem_get_info(cuda)[0] == free_before
+            assert _free_bytes_settled(cuda, free_before) == free_before
         assert torch.isfinite(y).all()
         assert rel(y, ref) < F32_RTOL
+        oracle = torch.tensor(O.attention_matvec(E_np, lam, x_np.astype(np.float64)))
+        assert rel(y.cpu(), oracle) < F32_RTOL
 
 
 def test_noalloc_rectangular_and_limit(cuda):
