@@ -104,6 +104,7 @@ struct K1tCfg {
   static constexpr uint32_t kOffBar = kOffCol + 4 * kTB * 4;  // barriers, TMEM slot, abort flag
   static constexpr uint32_t kSmemBytes = kOffBar + kNumBars * 8 + 16 + 1024;  // + alignment slack
   static_assert(kSmemBytes <= 227 * 1024, "shared memory budget");
+  static_assert(kSmemBytes > kTmemExclusiveSmem, "one TMEM-owning CTA per SM");
 };
 
 // Byte offset of TF32 element k of point row r inside a block variant

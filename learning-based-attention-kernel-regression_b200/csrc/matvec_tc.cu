@@ -770,8 +770,9 @@ cudaError_t launch_k2_t(const float* rows32, int64_t m, const float* cols32, con
                         float* Y, int64_t ldy, float* part, int* status, cudaStream_t s,
                         const int* gate) {
   const int S = k2_stages(N, TK, DP);
-  const size_t smem = k2_smem_bytes(N, S, TK, DP);
+  size_t smem = k2_smem_bytes(N, S, TK, DP);
   if (S < 2 || smem > 227 * 1024) return cudaErrorInvalidConfiguration;
+  if (smem <= kTmemExclusiveSmem) smem = kTmemExclusiveSmem + 1024;  // one TMEM owner per SM
   auto fn = k2_tc_matvec<DP, CLAMP, TK>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -818,8 +819,9 @@ cudaError_t launch_k2t_t(const uint8_t* rimg, int64_t m, const uint8_t* cimg, co
                          const int* gate) {
   const int AS = k2t_pslots(N);
   const int S = k2t_stages(N, AS);
-  const size_t smem = k2t_smem_bytes(N, S, AS);
+  size_t smem = k2t_smem_bytes(N, S, AS);
   if (S < 2 || smem > 227 * 1024) return cudaErrorInvalidConfiguration;
+  if (smem <= kTmemExclusiveSmem) smem = kTmemExclusiveSmem + 1024;  // one TMEM owner per SM
   auto fn = k2t_matvec<CLAMP, 32>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;

@@ -8,6 +8,15 @@
 
 namespace laker {
 
+// Every kernel of this library that allocates tensor memory takes all 512
+// TMEM columns of its SM (tcgen05.alloc blocks while they are taken).  Each
+// such kernel therefore keeps its shared memory above half of the SM's 228 KB,
+// so no two of them (the same kernel or two different ones, e.g. the engine's
+// operator and a variance product on another stream) are ever resident on
+// one SM at once: a CTA never waits in tcgen05.alloc for another CTA that
+// shares its SM.
+constexpr uint32_t kTmemExclusiveSmem = 116u * 1024u;
+
 // Shared-memory matrix descriptor of a K-major operand in a swizzled
 // canonical layout: 8-row core groups `sbo` bytes apart, layout code 2
 // (128-byte swizzle), 4 (64-byte swizzle) or 6 (32-byte swizzle), tiles

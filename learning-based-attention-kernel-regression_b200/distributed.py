@@ -164,7 +164,10 @@ class RowShard:
 class ShardedPreconditioner:
     """This rank's rows of the factored CCCP apply P = c^-1/2 I + Q W Q^T
     (laker/preconditioner.py:52-68 with W = V diag(l^-1/2 - c^-1/2) V^T
-    folded): Q_loc (rows x nr), W (nr x nr), c^-1/2, all FP64."""
+    folded): Q_loc (rows x nr), W (nr x nr), c^-1/2, held in FP64 but with Q
+    and W taken from the fused apply's FP32 factors (apply_factors()), so the
+    sharded apply carries the same FP32 rounding of Q and W as the
+    single-GPU apply."""
 
     def __init__(self, q_loc: torch.Tensor, w: torch.Tensor, inv_sqrt_iso: float) -> None:
         self.q = q_loc.to(torch.float64).contiguous()

@@ -212,43 +212,14 @@ class CCCPPreconditioner:
         clock.stop("qr")
 
         shrinkage = adaptive_shrinkage_rho(self.nr, n, self.gamma, self.base_rho)
-        reg_scale = 1.0 + self.gamma / n
-        iso = 1.0
-        qbm = torch.zeros(self.nr, self.nr, device=dev, dtype=dt)
-        eye = torch.eye(self.nr, device=dev, dtype=dt)
-        it = 0
-        for it in range(self.max_iter):
-            iso_prev = iso
-            qbm_prev = qbm.clone()
-            m_mat = eye * iso + qbm
-            # diag(R^T M^-1 R) by a Cholesky solve (M = c I + B is SPD); the
-            # reference forms it from eigh(M) (laker/preconditioner.py:207-225),
-            # which gives the same values at a few times the cost
-            chol, info = torch.linalg.cholesky_ex(m_mat)
-            if int(info.item()) == 0:
-                denom = (self.qr_r * torch.cholesky_solve(self.qr_r, chol)).sum(dim=0) + self.epsilon
-            else:
-                evals, evecs = eigh_stable(m_mat, eps=self.epsilon)
-                proj = evecs.T @ self.qr_r
-                inv_m_r = proj.T @ (evals.reciprocal().unsqueeze(-1) * proj)
-                denom = torch.diagonal(inv_m_r) + self.epsilon
-            weights = (n / self.nr) / denom
-            wrr = (self.qr_r * weights.unsqueeze(0)) @ self.qr_r.T
-            f_gamma = (wrr + self.gamma * eye) * (1.0 / reg_scale)
-            shrunk = torch.lerp(f_gamma, eye, shrinkage)
-            shrunk_iso = (1.0 - shrinkage) * self.gamma / reg_scale + shrinkage
-            trace = shrunk_iso * (n - self.nr) + shrunk.diagonal().sum()
-            scale = n / trace
-            iso = float(scale * shrunk_iso)
-            qbm = shrunk * scale
-            qbm.diagonal().sub_(iso)
-            iso_rel = abs(iso - iso_prev) / (abs(iso_prev) + 1e-12)
-            q_rel = (torch.norm(qbm - qbm_prev, p="fro") / (torch.norm(qbm_prev, p="fro") + 1e-12)).item()
-            if self.verbose and (it % 10 == 0 or max(iso_rel, q_rel) < self.tol):
-                logger.info("CCCP iter %d: isotropic_rel=%.3e, q_basis_rel=%.3e, isotropic_coef=%.6f",
-                            it, iso_rel, q_rel, iso)
-            if max(iso_rel, q_rel) < self.tol:
-                break
+        iso, qbm, iters = self._fixed_point_device(n, shrinkage)
+        if iso is None:
+            # M = c I + B was not positive definite at some iteration (not met
+            # on the configs): the reference's eigh formulation, one host
+            # synchronisation per iteration
+            iso, qbm, iters = self._fixed_point_eigh(n, shrinkage)
+        it = iters - 1
+        eye = torch.eye(self.nr, device=dev, dtype=torch.float64)
         self.cccp_iterations = it + 1
         self.isotropic_coef = iso
         self.q_basis_matrix = qbm
@@ -261,6 +232,87 @@ class CCCPPreconditioner:
         if self.verbose:
             logger.info("CCCP preconditioner built in %d iterations", it + 1)
         return self
+
+    def _fixed_point_device(self, n: int, shrinkage: float):
+        """The N_r x N_r CCCP fixed point (laker/preconditioner.py:207-273)
+        with its scalars, convergence test and iteration count kept on the
+        device: the state freezes at the iteration the reference stops at
+        (max(iso_rel, q_rel) < tol), and the host polls every 4 iterations
+        instead of once per iteration.  diag(R^T M^-1 R) comes from a Cholesky
+        solve (the reference's eigh gives the same quantity for SPD M).
+        Returns (c, B, iterations), or (None, None, 0) if a Cholesky
+        factorisation failed (M not positive definite)."""
+        dev, dt = self.device, torch.float64
+        nr = self.nr
+        reg_scale = 1.0 + self.gamma / n
+        eye = torch.eye(nr, device=dev, dtype=dt)
+        iso = torch.ones((), device=dev, dtype=dt)
+        qbm = torch.zeros(nr, nr, device=dev, dtype=dt)
+        active = torch.ones((), device=dev, dtype=torch.bool)
+        failed = torch.zeros((), device=dev, dtype=torch.bool)
+        iters = torch.zeros((), device=dev, dtype=torch.int64)
+        shrunk_iso = (1.0 - shrinkage) * self.gamma / reg_scale + shrinkage
+        for it in range(self.max_iter):
+            chol, info = torch.linalg.cholesky_ex(eye * iso + qbm)
+            failed |= info != 0
+            denom = (self.qr_r * torch.cholesky_solve(self.qr_r, chol)).sum(dim=0) + self.epsilon
+            weights = (n / nr) / denom
+            wrr = (self.qr_r * weights.unsqueeze(0)) @ self.qr_r.T
+            f_gamma = (wrr + self.gamma * eye) * (1.0 / reg_scale)
+            shrunk = torch.lerp(f_gamma, eye, shrinkage)
+            trace = shrunk_iso * (n - nr) + shrunk.diagonal().sum()
+            scale = n / trace
+            iso_new = scale * shrunk_iso
+            qbm_new = shrunk * scale
+            qbm_new.diagonal().sub_(iso_new)
+            iso_rel = (iso_new - iso).abs() / (iso.abs() + 1e-12)
+            q_rel = torch.norm(qbm_new - qbm, p="fro") / (torch.norm(qbm, p="fro") + 1e-12)
+            iso = torch.where(active, iso_new, iso)
+            qbm = torch.where(active, qbm_new, qbm)
+            iters = iters + active.to(torch.int64)
+            active = active & ~(torch.maximum(iso_rel, q_rel) < self.tol)
+            if it % 4 == 3 or it == self.max_iter - 1:
+                done, bad = bool((~active) | failed), bool(failed)
+                if self.verbose:
+                    logger.info("CCCP iter %d: isotropic_coef=%.6f (active=%s)", it,
+                                float(iso), bool(active))
+                if bad:
+                    return None, None, 0
+                if done:
+                    break
+        return float(iso), qbm, int(iters)
+
+    def _fixed_point_eigh(self, n: int, shrinkage: float):
+        """The fixed point with eigh-based diag(R^T M^-1 R), as the reference
+        computes it, synchronising once per iteration."""
+        dev, dt = self.device, torch.float64
+        reg_scale = 1.0 + self.gamma / n
+        iso = 1.0
+        qbm = torch.zeros(self.nr, self.nr, device=dev, dtype=dt)
+        eye = torch.eye(self.nr, device=dev, dtype=dt)
+        it = 0
+        for it in range(self.max_iter):
+            iso_prev = iso
+            qbm_prev = qbm.clone()
+            evals, evecs = eigh_stable(eye * iso + qbm, eps=self.epsilon)
+            proj = evecs.T @ self.qr_r
+            inv_m_r = proj.T @ (evals.reciprocal().unsqueeze(-1) * proj)
+            denom = torch.diagonal(inv_m_r) + self.epsilon
+            weights = (n / self.nr) / denom
+            wrr = (self.qr_r * weights.unsqueeze(0)) @ self.qr_r.T
+            f_gamma = (wrr + self.gamma * eye) * (1.0 / reg_scale)
+            shrunk = torch.lerp(f_gamma, eye, shrinkage)
+            shrunk_iso = (1.0 - shrinkage) * self.gamma / reg_scale + shrinkage
+            trace = shrunk_iso * (n - self.nr) + shrunk.diagonal().sum()
+            scale = n / trace
+            iso = float(scale * shrunk_iso)
+            qbm = shrunk * scale
+            qbm.diagonal().sub_(iso)
+            iso_rel = abs(iso - iso_prev) / (abs(iso_prev) + 1e-12)
+            q_rel = (torch.norm(qbm - qbm_prev, p="fro") / (torch.norm(qbm_prev, p="fro") + 1e-12)).item()
+            if max(iso_rel, q_rel) < self.tol:
+                break
+        return iso, qbm, it + 1
 
     # eigen-decomposition of c I + B (reference state attributes); a batched
     # build leaves it to be computed on first access

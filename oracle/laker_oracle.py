@@ -86,7 +86,7 @@ def attention_matvec(E, lam, X, clamp: bool = False, clamp_value: float = 700.0)
     X = np.asarray(X, dtype=np.float64)
     n = E.shape[0]
     lib = _c_lib()
-    if n > NUMPY_MAX_N and lib is not None:
+    if n > NUMPY_MAX_N and lib is not None and _narrow(X):
         return _c_matvec(lib, E, E, lam, X, clamp, clamp_value)
     return _np_matvec(E, E, lam, X, clamp, clamp_value, square=True)
 
@@ -97,9 +97,15 @@ def rect_matvec(Eq, E, X, clamp: bool = False, clamp_value: float = 700.0):
     E = np.ascontiguousarray(E, dtype=np.float64)
     X = np.asarray(X, dtype=np.float64)
     lib = _c_lib()
-    if max(Eq.shape[0], E.shape[0]) > NUMPY_MAX_N and lib is not None:
+    if max(Eq.shape[0], E.shape[0]) > NUMPY_MAX_N and lib is not None and _narrow(X):
         return _c_matvec(lib, Eq, E, 0.0, X, clamp, clamp_value)
     return _np_matvec(Eq, E, 0.0, X, clamp, clamp_value, square=False)
+
+
+def _narrow(X) -> bool:
+    """Few right-hand sides take the OpenMP C loop; wide blocks the blocked
+    numpy path, whose (rows x n) @ (n x k) products run as BLAS GEMMs."""
+    return X.ndim == 1 or X.shape[1] <= 8
 
 
 def _np_matvec(Er, Ec, lam, X, clamp, clamp_value, square):

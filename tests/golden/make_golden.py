@@ -1,9 +1,8 @@
 """Generate tests/golden/*.npz by running the LAKER reference package itself.
 
-Run in a checkout where the reference source is available (default
-/root/reference, or pass its path):
+Run where the reference source is available, passing its path:
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py /path/to/reference
 
 The fixtures pin the float64 oracle (oracle/laker_oracle.py) and the GPU
 path.  Inputs come from laker_b200.data.synthetic_field (CPU torch draws) and
@@ -22,7 +21,9 @@ import torch
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parent.parent
-REF = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+if len(sys.argv) < 2:
+    sys.exit(f"usage: python {Path(__file__).name} <path of the reference checkout>")
+REF = Path(sys.argv[1])
 sys.path.insert(0, str(REF))
 sys.path.insert(0, str(REPO))
 

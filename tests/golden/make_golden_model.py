@@ -3,7 +3,7 @@ LAKERRegressor.save (laker/persistence.py:74-137): a float64 fit on CPU at
 n = 300 (synthetic field, seed 0).  The persistence tests load it to check
 that a file written by the reference restores here.
 
-    python tests/golden/make_golden_model.py [/path/to/reference]
+    python tests/golden/make_golden_model.py /path/to/reference
 """
 
 from __future__ import annotations
@@ -15,7 +15,9 @@ import torch
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parent.parent
-REF = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+if len(sys.argv) < 2:
+    sys.exit(f"usage: python {Path(__file__).name} <path of the reference checkout>")
+REF = Path(sys.argv[1])
 sys.path.insert(0, str(REF))
 sys.path.insert(0, str(REPO))
 

@@ -263,3 +263,69 @@ def test_pcg_edge_cases(cuda):
     short = PreconditionedConjugateGradient(tol=1e-14, max_iter=3, verbose=False)
     short.solve(op.matvec, None, b)
     assert short.iterations == 3
+
+
+@pytest.mark.parametrize("k", [2, 5, 16])
+def test_narrow_multi_rhs_fp64_vs_oracle(cuda, k):
+    """FP64 multi-RHS products of at most 16 right-hand sides (64 x 16 tiles),
+    with and without a right-hand side B (the residual B - A X)."""
+    from laker_b200 import _lib
+
+    rng = np.random.default_rng(300 + k)
+    n = 2100
+    E = rng.standard_normal((n, 10)) * 0.5
+    X = rng.standard_normal((n, k))
+    B = rng.standard_normal((n, k))
+    p64 = _lib.pack_f64(torch.tensor(E, device=cuda))
+    Xt, Bt = torch.tensor(X, device=cuda), torch.tensor(B, device=cuda)
+    ref = O.attention_matvec(E, 0.07, X)
+    assert rel(_lib.attn_matvec_f64(p64, n, p64, n, 10, 0.07, 0, Xt), ref) < F64_RTOL
+    assert rel(_lib.attn_matvec_f64(p64, n, p64, n, 10, 0.07, 0, Xt, B=Bt), B - ref) < F64_RTOL
+
+
+_NARROW_CHILD = r"""
+import numpy as np, torch
+from oracle import laker_oracle as O
+from laker_b200 import _lib
+cuda = torch.device("cuda", 0)
+out = []
+for k in (2, 5, 16):
+    rng = np.random.default_rng(400 + k)
+    n = 1900
+    E = (rng.standard_normal((n, 10)) * 0.5).astype(np.float32)
+    X = rng.standard_normal((n, k))
+    p32 = _lib.pack_f32(torch.tensor(E, device=cuda))
+    p64 = _lib.pack_f64(torch.tensor(E, device=cuda))
+    Y = _lib.attn_matvec_f32(p32, n, p32, n, 10, 0.07, 0, torch.tensor(X, device=cuda, dtype=torch.float32))
+    Y64 = _lib.attn_matvec_f64(p64, n, p64, n, 10, 0.07, 0, torch.tensor(X, device=cuda))
+    ref = O.attention_matvec(E, 0.07, X)
+    out.append(np.linalg.norm(Y.double().cpu().numpy() - ref) / np.linalg.norm(ref))
+    np.save(f"_narrow_{k}.npy", Y64.cpu().numpy())
+print("WORST", max(out))
+"""
+
+
+def test_narrow_multi_rhs_cuda_core_paths(cuda, tmp_path):
+    """The CUDA-core FP32 multi-RHS kernel (LAKER_K2_TENSOR_CORES=0; the
+    switches are read once per process, hence child processes) against the
+    oracle, and the narrow 64 x 16 tiles against the wide ones
+    (LAKER_MULTI_NARROW=0): the same FP64 products."""
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parents[1]
+    results = {}
+    for narrow in ("1", "0"):
+        d = tmp_path / narrow
+        d.mkdir()
+        env = dict(os.environ, LAKER_K2_TENSOR_CORES="0", LAKER_MULTI_NARROW=narrow,
+                   PYTHONPATH=str(root))
+        out = subprocess.run([sys.executable, "-c", _NARROW_CHILD], cwd=d, env=env,
+                             capture_output=True, text=True, timeout=600)
+        assert out.returncode == 0, out.stderr[-2000:]
+        assert float(out.stdout.split("WORST")[-1]) < F32_RTOL
+        results[narrow] = {k: np.load(d / f"_narrow_{k}.npy") for k in (2, 5, 16)}
+    for k in (2, 5, 16):
+        assert np.linalg.norm(results["1"][k] - results["0"][k]) <= F64_RTOL * np.linalg.norm(results["0"][k])
