@@ -173,6 +173,14 @@ int laker_fp32_operator_kernel(int64_t n, int d);
  *                                which runs the failure path deterministically
  *                                without a fault or a hang. */
 #define LAKER_VARIANT_WAIT_LIMIT_US 6
+/*   LAKER_VARIANT_MULTI_FLASH_K  multi-RHS FP32 products of unclamped
+ *                                operators with at most this many right-hand
+ *                                sides take the flash-style tensor-core kernel
+ *                                (logits and P X on the tensor cores, P kept
+ *                                in tensor memory; chunks of 64 right-hand
+ *                                sides); 0 turns it off.  Default 0
+ *                                (environment LAKER_MULTI_FLASH_K). */
+#define LAKER_VARIANT_MULTI_FLASH_K 7
 int laker_set_variant(int which, int value);
 int laker_get_variant(int which);
 

@@ -491,6 +491,7 @@ VARIANT_K2_LOGITS_WIDE = 3
 VARIANT_SYM_MIN_BLOCKS = 4
 VARIANT_K1T_LOGITS = 5
 VARIANT_WAIT_LIMIT_US = 6
+VARIANT_MULTI_FLASH_K = 7
 
 
 def set_variant(which: int, value: int) -> int:

@@ -63,6 +63,27 @@ cudaError_t launch_k2(const float* rows32, int64_t m, const float* cols32, int64
                       int64_t ldy, uint8_t* img, int* status, cudaStream_t s,
                       const int* gate = nullptr);
 
+// Split, swizzled TF32 image of X (n x k) in 32-point tiles of N right-hand
+// sides (the multi-RHS kernels' B operand): chunk c, tile t at
+// (c * ntiles + t) * N * 256 bytes, [hi: N rows x 128 B][lo: N rows x 128 B]
+// in the 128-byte-swizzled K-major layout; points past n are zero.
+cudaError_t launch_pack_x32(const float* X, int64_t n, int64_t ldx, int k, int N, int64_t ntiles,
+                            uint8_t* img, const int* gate, cudaStream_t s);
+// Y = lam X + sum over `segs` segment partials (segs x m x k floats), in
+// segment order.
+cudaError_t launch_seg_reduce(const float* part, int segs, int64_t m, int k, float lam,
+                              const float* X, int64_t ldx, float* Y, int64_t ldy, const int* gate,
+                              cudaStream_t s);
+
+// ---- flash-style multi-RHS FP32 matvec (matvec_flash.cu) --------------------
+// Whether a product of k right-hand sides takes it (unclamped operators, k up
+// to LAKER_VARIANT_MULTI_FLASH_K), and its workspace.
+bool k2f_enabled(int k, int clamp);
+size_t k2f_workspace_bytes(int64_t m, int64_t n, int k, bool same_points);
+cudaError_t launch_k2f(const float* rows32, int64_t m, const float* cols32, int64_t n, int d,
+                       float lam, const float* X, int64_t ldx, int k, float* Y, int64_t ldy,
+                       uint8_t* ws, int* status, cudaStream_t s, const int* gate = nullptr);
+
 // ---- multi-RHS solve and preconditioner apply (pcg_multi.cu) ----------------
 size_t pcg_multi_workspace_bytes(int64_t n, int d, int nr, int k);
 int pcg_solve_multi(const laker_operator* op, const laker_precond* pc, const double* B, int k,
@@ -84,6 +105,7 @@ cudaError_t set_wait_limit_f64(unsigned long long ns);
 cudaError_t set_wait_limit_sym(unsigned long long ns);
 cudaError_t set_wait_limit_symtc(unsigned long long ns);
 cudaError_t set_wait_limit_tc(unsigned long long ns);
+cudaError_t set_wait_limit_flash(unsigned long long ns);
 
 // Y[i, c] = NaN for i < m, c < k when *status != 0: the outputs of a product
 // whose kernel recorded a device-side failure (a bounded wait that expired)

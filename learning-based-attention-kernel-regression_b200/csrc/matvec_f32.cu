@@ -508,8 +508,11 @@ using namespace laker;
 extern "C" size_t laker_matvec_workspace_bytes(int64_t m, int64_t n, int d, int k, int precision) {
   if (m < 0 || n < 0 || d < 1 || d > 16 || k < 1) return 0;
   if (k > 1) {
-    // the tensor-core path stages X as split, swizzled TF32 tiles
-    return kWsHeader + (k2_use_tensor_cores() && n > 0 ? (size_t)round_up((int64_t)k2_image_bytes(m, n, k), 256) : 0);
+    // the tensor-core paths stage X as split, swizzled TF32 tiles (and the
+    // flash-style kernel the split-FP16 operand images of the points)
+    size_t b = k2_use_tensor_cores() && n > 0 ? (size_t)round_up((int64_t)k2_image_bytes(m, n, k), 256) : 0;
+    const size_t f = n > 0 && m > 0 ? k2f_workspace_bytes(m, n, k, false) : 0;
+    return kWsHeader + (b > f ? b : f);
   }
   const SegPlan p = precision == 64 ? k4_plan(m, n, d) : k1_plan(m, n, d);
   size_t bytes = (size_t)p.S * (size_t)m * sizeof(double);
@@ -538,7 +541,12 @@ extern "C" int laker_attn_matvec_f32(const float* rows32, int64_t m, const float
   cudaError_t e = cudaMemsetAsync(&hdr->status, 0, sizeof(int), s);
   if (e != cudaSuccess) return fail_cuda(e);
   if (k > 1) {
-    if (k2_use_tensor_cores() && n > 0) {
+    if (n > 0 && k2f_enabled(k, clamp)) {
+      uint8_t* img = reinterpret_cast<uint8_t*>(workspace) + kWsHeader;
+      e = launch_k2f(rows32, m, cols32, n, d, (m == n) ? lam : 0.0f, X, ldx, k, Y, ldy, img,
+                     &hdr->status, s);
+      if (e == cudaSuccess) e = launch_poison_on_status(&hdr->status, Y, m, k, ldy, s);
+    } else if (k2_use_tensor_cores() && n > 0) {
       uint8_t* img = reinterpret_cast<uint8_t*>(workspace) + kWsHeader;
       e = launch_k2(rows32, m, cols32, n, d, clamp, (m == n) ? lam : 0.0f, X, ldx, k, Y, ldy, img,
                     &hdr->status, s);

@@ -937,4 +937,24 @@ cudaError_t launch_k2(const float* rows32, int64_t m, const float* cols32, int64
 
 cudaError_t set_wait_limit_tc(unsigned long long ns) { return set_wait_limit_this_unit(ns); }
 
+cudaError_t launch_pack_x32(const float* X, int64_t n, int64_t ldx, int k, int N, int64_t ntiles,
+                            uint8_t* img, const int* gate, cudaStream_t s) {
+  const int64_t total = ntiles * 32 * ceil_div(k, N) * N;
+  int64_t g = ceil_div(total, 256);
+  if (g > (int64_t)sm_count() * 16) g = (int64_t)sm_count() * 16;
+  if (g < 1) g = 1;
+  k2_pack_x<32><<<(unsigned)g, 256, 0, s>>>(X, n, ldx, k, N, ntiles, img, gate);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_seg_reduce(const float* part, int segs, int64_t m, int k, float lam,
+                              const float* X, int64_t ldx, float* Y, int64_t ldy, const int* gate,
+                              cudaStream_t s) {
+  int64_t g = ceil_div(m * (int64_t)k, 256);
+  if (g > (int64_t)sm_count() * 16) g = (int64_t)sm_count() * 16;
+  if (g < 1) g = 1;
+  k2_reduce_kernel<<<(unsigned)g, 256, 0, s>>>(part, segs, m, k, lam, X, ldx, Y, ldy, gate);
+  return cudaGetLastError();
+}
+
 }  // namespace laker

@@ -663,7 +663,12 @@ MpcgWs carve_multi(void* base, int64_t n, int k, int nr) {
   w.Z = reinterpret_cast<float*>(take(nk * sizeof(float)));
   w.bp = reinterpret_cast<double*>(take((size_t)3 * g.gx * (size_t)k * sizeof(double)));
   w.pscratch = nr > 0 ? take(precond_multi_scratch_bytes(n, nr, k)) : nullptr;
-  w.img = k2_use_tensor_cores() ? reinterpret_cast<uint8_t*>(take(k2_image_bytes(n, n, k))) : nullptr;
+  {
+    // operator workspace: the tensor-core multi-RHS kernels' operand images
+    const size_t b2 = k2_use_tensor_cores() ? k2_image_bytes(n, n, k) : 0;
+    const size_t bf = k2f_workspace_bytes(n, n, k, true);
+    w.img = reinterpret_cast<uint8_t*>(take(b2 > bf ? b2 : bf));
+  }
   w.bytes = off;
   return w;
 }
@@ -752,13 +757,19 @@ int pcg_solve_multi(const laker_operator* op, const laker_precond* pc, const dou
   // ---- iterations ------------------------------------------------------------
   auto iteration = [&](cudaStream_t cs) -> cudaError_t {
     cudaError_t ee;
-    if (w.img)
+    if (k2f_enabled(k, op->clamp)) {
+      ee = launch_k2f(op->packed32, n, op->packed32, n, d, lam32, w.P, k, k, w.AP, k, w.img, dstatus,
+                      cs, &w.st->active);
+      launches += 4;
+    } else if (k2_use_tensor_cores()) {
       ee = launch_k2(op->packed32, n, op->packed32, n, d, op->clamp, lam32, w.P, k, k, w.AP, k, w.img,
                      dstatus, cs, &w.st->active);
-    else
+      launches += 3;
+    } else {
       ee = launch_multi_f32(op->packed32, n, op->packed32, n, d, lam32, op->clamp, w.P, k, k, w.AP, k,
                             cs, &w.st->active);
-    launches += w.img ? 3 : 1;
+      launches += 1;
+    }
     if (ee != cudaSuccess) return ee;
     mp_after_matvec_kernel<<<cgrid, kMT, 0, cs>>>(w.P, w.AP, n, k, w.bp, w.st, w.cols, dstatus);
     mp_update_xr_kernel<<<cgrid, kMT, 0, cs>>>(w.P, w.AP, X, w.R, n, k, w.bp, w.st, w.cols);

@@ -10,8 +10,8 @@
 namespace laker {
 namespace {
 
-constexpr int kNumVariants = 7;
-std::atomic<int> g_variant[kNumVariants] = {{-1}, {-1}, {-1}, {-1}, {-1}, {-1}, {-1}};
+constexpr int kNumVariants = 8;
+std::atomic<int> g_variant[kNumVariants] = {{-1}, {-1}, {-1}, {-1}, {-1}, {-1}, {-1}, {-1}};
 
 // Default bounded-wait limit: 2 s.
 constexpr int kWaitLimitDefaultUs = 2000000;
@@ -40,6 +40,14 @@ int variant_default(int which) {
     return (e && e[0] == '0') ? 0 : 1;
   }
   if (which == LAKER_VARIANT_WAIT_LIMIT_US) return kWaitLimitDefaultUs;
+  if (which == LAKER_VARIANT_MULTI_FLASH_K) {
+    const char* e = getenv("LAKER_MULTI_FLASH_K");
+    if (e && e[0]) {
+      const int v = atoi(e);
+      if (v >= 0 && v <= 1 << 20) return v;
+    }
+    return 0;
+  }
   const char* e = getenv("LAKER_K2_LOGITS_TC");
   return (e && e[0] == '1') ? 1 : 0;
 }
@@ -49,6 +57,7 @@ bool variant_valid(int which, int value) {
   if (which == LAKER_VARIANT_SYM_MIN_BLOCKS) return value >= 0 && value <= 64;
   if (which == LAKER_VARIANT_K1T_LOGITS) return value == 0 || value == 1;
   if (which == LAKER_VARIANT_WAIT_LIMIT_US) return value >= 0 && value <= kWaitLimitDefaultUs;
+  if (which == LAKER_VARIANT_MULTI_FLASH_K) return value >= 0 && value <= 1 << 20;
   return value == 0 || value == 1;
 }
 
@@ -58,7 +67,7 @@ cudaError_t apply_wait_limit(int us) {
   const unsigned long long ns = (unsigned long long)us * 1000ull;
   cudaError_t (*const setters[])(unsigned long long) = {set_wait_limit_f32, set_wait_limit_f64,
                                                         set_wait_limit_sym, set_wait_limit_symtc,
-                                                        set_wait_limit_tc};
+                                                        set_wait_limit_tc, set_wait_limit_flash};
   for (auto f : setters) {
     const cudaError_t e = f(ns);
     if (e != cudaSuccess) return e;
