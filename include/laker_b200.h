@@ -177,8 +177,8 @@ int laker_fp32_operator_kernel(int64_t n, int d);
  *                                operators with at most this many right-hand
  *                                sides take the flash-style tensor-core kernel
  *                                (logits and P X on the tensor cores, P kept
- *                                in tensor memory; chunks of 64 right-hand
- *                                sides); 0 turns it off.  Default 0
+ *                                in tensor memory; chunks of 32 right-hand
+ *                                sides); 0 turns it off.  Default 32
  *                                (environment LAKER_MULTI_FLASH_K). */
 #define LAKER_VARIANT_MULTI_FLASH_K 7
 int laker_set_variant(int which, int value);

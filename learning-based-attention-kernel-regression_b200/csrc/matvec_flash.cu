@@ -1,5 +1,5 @@
 // Flash-style multi-RHS FP32 attention-kernel matvec on the tensor cores:
-//   Y = [lam X +] exp(E_rows E_cols^T) X        (X: n x k, k <= 64 per chunk)
+//   Y = [lam X +] exp(E_rows E_cols^T) X        (X: n x k, k <= 32 per chunk)
 // for operators whose Gram entries need no clamp.
 //
 // The shape is FlashAttention's forward without the softmax normalisation
@@ -17,23 +17,29 @@
 //                      memory: P_hi X_hi + P_hi X_lo + P_lo X_hi (~2^-21
 //                      relative per product, as FP32 entries; plain TF32
 //                      would perturb A by more than lambda), FP32 accumulation
-//                      in TMEM.
+//                      in TMEM.  The X tile stores X_hi's N rows right above
+//                      X_lo's, so P_hi [X_hi | X_lo] is one MMA of width 2 N
+//                      and P_lo X_hi a second one into the first N columns:
+//                      two MMAs per K step; the output is the sum of the two
+//                      column halves.
 // Per kernel entry the CUDA cores do one ex2 and a few conversions: the kernel
 // is bound by the MUFU ex2 rate, where the CUDA-core-logit multi-RHS kernel
 // (k2_tc_matvec) spends d FMAs, embedding loads and a shared-memory write per
-// entry.  Each entry is evaluated once per chunk of up to 64 right-hand sides.
+// entry.  Each entry is evaluated once per chunk of up to 32 right-hand sides.
 //
 // Work items: (row tile, RHS chunk, column segment), rows fastest, taken by a
 // persistent grid; segments of the column range keep every SM busy and their
 // partial outputs are added in a fixed order (launch_seg_reduce), so the
 // result does not depend on scheduling.
 //
-// Roles in a CTA of 576 threads (one CTA per SM: 448 TMEM columns of the 512
-// taken, more than half of the SM's shared memory):
-//   warps 0-15 epilogue: warp w owns TMEM lanes 32 (w & 3) .. + 31 and 16 of a
-//             slab's 64 columns (w >> 2): exp2 and the split into P; the four
-//             warps of column group 0 also read the item's accumulators and
-//             write its output rows;
+// Roles in a CTA of 576 threads (one CTA per SM: all 512 TMEM columns taken,
+// more than half of the SM's shared memory):
+//   warps 0-15 epilogue, two groups of eight that take alternate slabs (two
+//             slabs' exp2 in flight, so one group's TMEM and barrier latencies
+//             hide behind the other's work): warp w owns TMEM lanes
+//             32 (w & 3) .. + 31 and 32 of a slab's 64 columns ((w >> 2) & 1):
+//             exp2 and the split into P; the four warps of group 0, column
+//             half 0 also read the item's accumulators and write its rows;
 //   warp 16   copies: the item's row operands (double-buffered), per slab the
 //             column operands and the X tiles (S stages);
 //   warp 17   MMA (lane 0): the slab's logits one slab ahead of its P X
@@ -55,10 +61,11 @@ constexpr int kFEpiWarps = 16;
 constexpr int kFThreads = kFEpiWarps * 32 + 64;   // + copy warp + MMA warp
 constexpr int kFCopyWarp = kFEpiWarps, kFMmaWarp = kFEpiWarps + 1;
 constexpr int kFBufs = 3;                         // TMEM logit / P buffers
-constexpr int kFMaxN = 64;                        // right-hand sides per chunk
+constexpr int kFMaxN = 32;                        // right-hand sides per chunk
+constexpr int kFGroupWarps = 8;                   // epilogue warps per slab group
 constexpr int kFMaxStages = 8;
 // TMEM columns: buffer b holds S, then P_hi, at [128 b, 128 b + 64) and P_lo
-// at [128 b + 64, 128 b + 128); accumulator a at [384 + 64 a, + N).
+// at [128 b + 64, 128 b + 128); accumulator a at [384 + 64 a, + 2 N).
 constexpr uint32_t kFAccCol = 128u * kFBufs;
 // Split-FP16 operand image of k1t_pack: per 512-point block 128 KB, row side
 // (H, L, Hs) then column side (H, L, Hs), 16 KB per variant, 32 bytes per
@@ -74,7 +81,7 @@ constexpr uint32_t kFSBO16 = 8u * 32u;             // 8-row core group, FP16 ope
 constexpr uint32_t kFLayout16 = 6u;                // SWIZZLE_32B
 constexpr uint32_t kFSBO32 = 8u * 128u;            // 8-row core group, X tiles
 constexpr uint32_t kFLayout128 = 2u;               // SWIZZLE_128B
-static_assert(kFAccCol + 2 * kFMaxN <= 512, "TMEM budget");
+static_assert(kFAccCol + 2 * (2 * kFMaxN) <= 512, "TMEM budget");
 
 struct K2fWork {
   int64_t rtiles;  // row tiles of 128
@@ -138,7 +145,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
     for (int i = 0; i < kFBufs; ++i) {
       mbar_init(&s_full[i], 1);
       mbar_init(&s_empty[i], 1);
-      mbar_init(&p_full[i], kFEpiWarps);  // one arrival per epilogue warp
+      mbar_init(&p_full[i], kFGroupWarps);  // one arrival per warp of the slab's group
     }
     mbar_init(drain, 1);
     *abort = 0;
@@ -201,6 +208,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
     if (lane == 0) {
       const uint32_t idesc_s = f16_idesc_mn(kFRows, kFSlab);
       const uint32_t idesc_p = tf32_idesc_mn(kFRows, N);
+      const uint32_t idesc_p2 = tf32_idesc_mn(kFRows, 2 * N);
       int64_t g = 0, ni = 0;
       // the logits of global slab gg (row operands of buffer ab), into its buffer
       auto logits = [&](int64_t gg, int ab) -> bool {
@@ -231,7 +239,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
         if (!wait_or_abort(&a_full[ab], (uint32_t)((ni >> 1) & 1), status, abort)) break;
         if (!wait_or_abort(&acc_empty[ab], (uint32_t)(((ni >> 1) & 1) ^ 1), status, abort)) break;
         tc_fence_after();
-        const uint32_t dacc = tmem_base + kFAccCol + (uint32_t)(ab * kFMaxN);
+        const uint32_t dacc = tmem_base + kFAccCol + (uint32_t)(ab * 2 * kFMaxN);
         bool ok = logits(g, ab);
         for (int64_t s = s0; ok && s < s1; ++s, ++g) {
           if (s + 1 < s1 && !logits(g + 1, ab)) {
@@ -250,12 +258,10 @@ __global__ void __launch_bounds__(kFThreads, 1)
           for (int kk = 0; kk < kFSlab / 8; ++kk) {
             // X tile kk / 4, K step kk % 4 (32 bytes inside the swizzled row)
             const uint32_t xhi = xs + (uint32_t)((kk >> 2) * 256 * N) + (uint32_t)((kk & 3) * 32);
-            const uint32_t xlo = xhi + (uint32_t)(128 * N);
             const uint64_t bhi = kmajor_desc_raw(xhi, kFSBO32, kFLayout128);
-            const uint64_t blo = kmajor_desc_raw(xlo, kFSBO32, kFLayout128);
             const uint32_t acc = (s > s0 || kk > 0) ? 1u : 0u;
-            mma_tf32_ts(dacc, phi + 8u * kk, bhi, idesc_p, acc);
-            mma_tf32_ts(dacc, phi + 8u * kk, blo, idesc_p, 1u);
+            // D[:, 0:2N] += P_hi [X_hi | X_lo];  D[:, 0:N] += P_lo X_hi
+            mma_tf32_ts(dacc, phi + 8u * kk, bhi, idesc_p2, acc);
             mma_tf32_ts(dacc, plo + 8u * kk, bhi, idesc_p, 1u);
           }
           mma_commit(&s_empty[buf]);
@@ -268,7 +274,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
     }
   } else {
     // ---- epilogue (warps 0-15) ----------------------------------------------------
-    const int q = warp & 3, cg = warp >> 2;
+    const int q = warp & 3, ch2 = (warp >> 2) & 1, grp = warp >> 3;
     const uint32_t lane_off = (uint32_t)(q * 32) << 16;
     int64_t g = 0, ni = 0;
     bool dead = false;
@@ -277,32 +283,37 @@ __global__ void __launch_bounds__(kFThreads, 1)
       int ch, sg;
       item_of(it, &rt, &ch, &sg, &s0, &s1);
       for (int64_t s = s0; s < s1; ++s, ++g) {
+        if ((int)(g & 1) != grp) continue;  // the other group's slab
         const int buf = (int)(g % kFBufs);
         if (!warp_wait_or_abort(&s_full[buf], (uint32_t)((g / kFBufs) & 1), status, abort, lane)) {
           dead = true;
           break;
         }
         tc_fence_after();
-        const uint32_t ts = tmem_base + lane_off + (uint32_t)(buf * 128 + cg * 16);
-        float v[16];
-        tmem_ld16(ts, v);
-        uint32_t hi[16], lo[16];
+        const uint32_t ts = tmem_base + lane_off + (uint32_t)(buf * 128 + ch2 * 32);
+        float v[32];
+        tmem_ld32(ts, v);
 #pragma unroll
-        for (int u = 0; u < 16; ++u) {
-          const float p = ex2_approx(v[u]);
-          hi[u] = to_tf32(p);
-          lo[u] = to_tf32(p - __uint_as_float(hi[u]));
+        for (int h = 0; h < 2; ++h) {
+          uint32_t hi[16], lo[16];
+#pragma unroll
+          for (int u = 0; u < 16; ++u) {
+            const float p = ex2_approx(v[16 * h + u]);
+            hi[u] = to_tf32(p);
+            lo[u] = to_tf32(p - __uint_as_float(hi[u]));
+          }
+          tmem_st16(ts + (uint32_t)(16 * h), hi);
+          tmem_st16(ts + 64u + (uint32_t)(16 * h), lo);
         }
-        tmem_st16(ts, hi);
-        tmem_st16(ts + 64u, lo);
         tmem_st_wait();
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(&p_full[buf]);
       }
       if (dead) break;
-      if (cg == 0) {
-        // the item's accumulators: rows of lane quadrant q, all N columns
+      if (grp == 0 && ch2 == 0) {
+        // the item's accumulators: rows of lane quadrant q; the output is the
+        // sum of the two column halves
         const int ab = (int)(ni & 1);
         if (!warp_wait_or_abort(&acc_full[ab], (uint32_t)((ni >> 1) & 1), status, abort, lane)) {
           dead = true;
@@ -310,18 +321,20 @@ __global__ void __launch_bounds__(kFThreads, 1)
         }
         tc_fence_after();
         const int64_t r = rt * kFRows + q * 32 + lane;
+        const uint32_t da = tmem_base + lane_off + kFAccCol + (uint32_t)(ab * 2 * kFMaxN);
         for (int c0 = 0; c0 < N; c0 += 16) {
-          float o[16];
-          tmem_ld16(tmem_base + lane_off + kFAccCol + (uint32_t)(ab * kFMaxN + c0), o);
+          float o[16], o2[16];
+          tmem_ld16x2(da + (uint32_t)c0, da + (uint32_t)(N + c0), o, o2);
           if (r < m) {
 #pragma unroll
             for (int u = 0; u < 16; ++u) {
               const int col = ch * N + c0 + u;
               if (col < k) {
+                const float val = o[u] + o2[u];
                 if (wk.segs == 1)
-                  Y[r * ldy + col] = o[u] + (lam != 0.0f ? lam * X[r * ldx + col] : 0.0f);
+                  Y[r * ldy + col] = val + (lam != 0.0f ? lam * X[r * ldx + col] : 0.0f);
                 else
-                  part[((int64_t)sg * m + r) * k + col] = o[u];
+                  part[((int64_t)sg * m + r) * k + col] = val;
               }
             }
           }
@@ -356,7 +369,8 @@ __global__ void __launch_bounds__(kFThreads, 1)
   }
 }
 
-// Right-hand sides per chunk: up to 64, a multiple of 16 (the MMA's N).
+// Right-hand sides per chunk: up to 32, a multiple of 16 (the MMA's N; the
+// stacked P_hi [X_hi | X_lo] product is 2 N wide).
 int k2f_chunk_cols(int k) { return (int)round_up(k < kFMaxN ? k : kFMaxN, 16); }
 
 int k2f_stages(int N) {

@@ -46,7 +46,10 @@ int variant_default(int which) {
       const int v = atoi(e);
       if (v >= 0 && v <= 1 << 20) return v;
     }
-    return 0;
+    // measured on B200 (n = 50k, k = 16: 3.73 vs 7.75 ms for the CUDA-core-
+    // logit kernel; n = 20k, k = 16: 0.70 vs 1.34 ms); wider products (one
+    // exp2 per entry per chunk of 32) are faster on the CUDA-core-logit kernel
+    return 32;
   }
   const char* e = getenv("LAKER_K2_LOGITS_TC");
   return (e && e[0] == '1') ? 1 : 0;

@@ -31,6 +31,16 @@ def _with_flash(enabled):
     return _lib.set_variant(_lib.VARIANT_MULTI_FLASH_K, 1024 if enabled else 0)
 
 
+@pytest.fixture(autouse=True)
+def flash_on(cuda):
+    """Every test of this file runs with the flash kernel selected for up to
+    1024 right-hand sides (the tests that compare switch it off locally)."""
+    from laker_b200 import _lib
+    prev = _with_flash(True)
+    yield
+    _lib.set_variant(_lib.VARIANT_MULTI_FLASH_K, prev)
+
+
 @pytest.mark.parametrize("n,k", [(1, 2), (31, 5), (65, 16), (257, 17), (700, 64), (1500, 100),
                                  (2048, 256), (3000, 16), (4100, 512)])
 def test_flash_square_matvec(cuda, n, k):
@@ -106,9 +116,16 @@ def test_flash_config_embeddings_large_n_rows(cuda):
     op = AttentionKernelOperator(E, lambda_reg=1e-2)
     rng = np.random.default_rng(5)
     X = rng.standard_normal((n, k)).astype(np.float32)
-    Y = op.matvec(torch.tensor(X, device=cuda)).double().cpu().numpy()
+    Xt = torch.tensor(X, device=cuda)
+    Y = op.matvec(Xt).double().cpu().numpy()
+    _with_flash(False)
+    Yk2 = op.matvec(Xt).double().cpu().numpy()
     rows = np.sort(rng.choice(n, 1024, replace=False))
     E64 = E.double().cpu().numpy()
     ref = O.rect_matvec(E64[rows], E64, X.astype(np.float64)) + 1e-2 * X[rows]
     err = np.linalg.norm(Y[rows] - ref, axis=0) / np.linalg.norm(ref, axis=0)
-    assert err.max() < TC_RTOL
+    err_k2 = np.linalg.norm(Yk2[rows] - ref, axis=0) / np.linalg.norm(ref, axis=0)
+    # rows are sums of 50k entries of ~1e-6 relative error against random
+    # signs (|K| |x| / |K x| ~ sqrt(n)): ~1e-4 per column for either kernel
+    assert err.max() < 3e-4
+    assert err.max() < 2.0 * err_k2.max() + 2e-5
