@@ -35,11 +35,36 @@ namespace {
 
 constexpr int T = kVecThreads;
 
+// Grid of the kernels that finish an operator application (each row adds the
+// partial sums of its block pairs, ~n / 512 loads): one row per thread, up to
+// 4 CTAs per SM, so that enough loads are in flight.
+int fin_grid(int64_t n) {
+  int64_t g = ceil_div(n, T);
+  const int64_t cap = 4 * (int64_t)sm_count();
+  if (g > cap) g = cap;
+  return (int)(g < 1 ? 1 : g);
+}
+
 int vec_grid(int64_t n) {
   int64_t g = ceil_div(n, T * 4);
   const int64_t cap = 2 * (int64_t)sm_count();
   if (g > cap) g = cap;
   return (int)(g < 1 ? 1 : g);
+}
+
+// Fixed-order total of the NQ per-block partials bp[NQ * b + q] over the
+// grid, computed by the whole (last) block: thread t adds blocks t, t + T, ...
+// in order, then a fixed shuffle tree and warp order.  Result in thread 0.
+// (One thread walking every block's partial serialises on the L2 latency.)
+template <int NQ>
+__device__ __forceinline__ void grid_total(const double* bp, double (&out)[NQ], double* scratch) {
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) out[q] = 0.0;
+  for (unsigned int b = threadIdx.x; b < gridDim.x; b += T) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) out[q] += __ldcg(bp + (int64_t)NQ * b + q);
+  }
+  block_sum<T, NQ>(out, scratch);
 }
 
 // x = 0 (unless warm start), r = b, |b| -> bnorm, tol_abs, rmax.
@@ -58,10 +83,10 @@ __global__ void __launch_bounds__(T)
   block_sum<T, 1>(v, s_red);
   if (threadIdx.x == 0) blockpart[blockIdx.x] = v[0];
   if (!arrive_last_block(&st->counters[kCtrBnorm])) return;
+  double tot[1];
+  grid_total<1>(blockpart, tot, s_red);
   if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (unsigned int k = 0; k < gridDim.x; ++k) t += __ldcg(blockpart + k);
-    const double bn = sqrt(t);
+    const double bn = sqrt(tot[0]);
     st->bnorm = bn;
     st->tol_abs = tol * bn;
     st->rnorm = bn;
@@ -111,13 +136,10 @@ __global__ void __launch_bounds__(T)
     blockpart[3 * blockIdx.x + 2] = v[2];
   }
   if (!arrive_last_block(&st->counters[kCtrMatvec])) return;
+  double tot[3];
+  grid_total<3>(blockpart, tot, s_red);
   if (threadIdx.x == 0) {
-    double pap = 0.0, pp = 0.0, aa = 0.0;
-    for (unsigned int k = 0; k < gridDim.x; ++k) {
-      pap += __ldcg(blockpart + 3 * k + 0);
-      pp += __ldcg(blockpart + 3 * k + 1);
-      aa += __ldcg(blockpart + 3 * k + 2);
-    }
+    const double pap = tot[0], pp = tot[1], aa = tot[2];
     st->pAp = pap;
     if (status_failed(dstatus)) {
       // the operator kernel recorded a device-side failure: its partials are
@@ -159,10 +181,10 @@ __global__ void __launch_bounds__(T)
   block_sum<T, 1>(v, s_red);
   if (threadIdx.x == 0) blockpart[blockIdx.x] = v[0];
   if (!arrive_last_block(&st->counters[kCtrUpdate])) return;
+  double tot[1];
+  grid_total<1>(blockpart, tot, s_red);
   if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (unsigned int k = 0; k < gridDim.x; ++k) t += __ldcg(blockpart + k);
-    const double rn = sqrt(t);
+    const double rn = sqrt(tot[0]);
     st->rnorm = rn;
     st->iter += 1;
     // Reliable-update trigger against the running maximum of the recurrence
@@ -208,10 +230,10 @@ __global__ void __launch_bounds__(T)
   block_sum<T, 1>(v, s_red);
   if (threadIdx.x == 0) blockpart[blockIdx.x] = v[0];
   if (!arrive_last_block(&st->counters[kCtrResid])) return;
+  double tot[1];
+  grid_total<1>(blockpart, tot, s_red);
   if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (unsigned int k = 0; k < gridDim.x; ++k) t += __ldcg(blockpart + k);
-    const double rn = sqrt(t);
+    const double rn = sqrt(tot[0]);
     st->rnorm = rn;
     st->true_rnorm = rn;
     st->rmax = rn;
@@ -260,9 +282,10 @@ __global__ void __launch_bounds__(T)
   block_sum<T, 1>(v, s_red);
   if (threadIdx.x == 0) blockpart[blockIdx.x] = v[0];
   if (!arrive_last_block(&st->counters[kCtrExpand])) return;
+  double tot[1];
+  grid_total<1>(blockpart, tot, s_red);
   if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (unsigned int k = 0; k < gridDim.x; ++k) t += __ldcg(blockpart + k);
+    const double t = tot[0];
     if (init) {
       st->rz = t;
       st->beta = 0.0;
@@ -359,7 +382,8 @@ PcgWs carve(void* base, int64_t n, int d, int nr) {
     return q;
   };
   const SegPlan p1 = k1_plan(n, n, d), p4 = k4_plan(n, n, d);
-  const int G = vec_grid(n) > precond_grid() ? vec_grid(n) : precond_grid();
+  int G = vec_grid(n) > precond_grid() ? vec_grid(n) : precond_grid();
+  if (fin_grid(n) > G) G = fin_grid(n);
   w.hdr = reinterpret_cast<WsHeader*>(take(kWsHeader));
   w.st = reinterpret_cast<PcgState*>(take(sizeof(PcgState)));
   w.r = reinterpret_cast<double*>(take(n * sizeof(double)));
@@ -420,7 +444,7 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
   const SymPlan sp = tc ? k1t_plan(n) : k1s_plan(n, d);
   double* sym_row = w.part32;
   float* sym_col = sym_colpart_ptr<float>(w.part32, sp);
-  const int G = vec_grid(n), Gp = precond_grid_for(n);
+  const int G = vec_grid(n), Gp = precond_grid_for(n), Gf = fin_grid(n);
   int* dstatus = &w.hdr->status;
   const bool sym64 = k4_use_symmetric();
   const SymPlan sp64 = k4s_plan(n, d);
@@ -432,12 +456,12 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
     if (sym64) {
       ee = launch_k4s(op->packed64, n, d, op->clamp, X, row64, col64, sp64, dstatus, gate, cs);
       if (ee == cudaSuccess)
-        pcg_after_residual_kernel<true><<<G, T, 0, cs>>>(nullptr, 0, sp64, row64, col64, B, X, w.r,
+        pcg_after_residual_kernel<true><<<Gf, T, 0, cs>>>(nullptr, 0, sp64, row64, col64, B, X, w.r,
                                                          n, init, w.blockpart, w.st);
     } else {
       ee = launch_k4(op->packed64, n, op->packed64, n, d, op->clamp, X, w.part64, p4, dstatus, gate, cs);
       if (ee == cudaSuccess)
-        pcg_after_residual_kernel<false><<<G, T, 0, cs>>>(w.part64, p4.S, sp64, nullptr, nullptr, B,
+        pcg_after_residual_kernel<false><<<Gf, T, 0, cs>>>(w.part64, p4.S, sp64, nullptr, nullptr, B,
                                                           X, w.r, n, init, w.blockpart, w.st);
     }
     return ee;
@@ -524,10 +548,10 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
     }
     if (timed) t32.end(cs);
     if (sym)
-      pcg_after_matvec_kernel<true><<<G, T, 0, cs>>>(w.part32, 0, sp, sym_row, sym_col, w.p, w.Ap, n,
+      pcg_after_matvec_kernel<true><<<Gf, T, 0, cs>>>(w.part32, 0, sp, sym_row, sym_col, w.p, w.Ap, n,
                                                      w.blockpart, w.st, dstatus);
     else
-      pcg_after_matvec_kernel<false><<<G, T, 0, cs>>>(w.part32, p1.S, sp, nullptr, nullptr, w.p, w.Ap,
+      pcg_after_matvec_kernel<false><<<Gf, T, 0, cs>>>(w.part32, p1.S, sp, nullptr, nullptr, w.p, w.Ap,
                                                       n, w.blockpart, w.st, dstatus);
     pcg_update_xr_kernel<<<G, T, 0, cs>>>(w.p, w.Ap, X, w.r, n, w.blockpart, w.st);
     if (timed) t64.begin(cs);

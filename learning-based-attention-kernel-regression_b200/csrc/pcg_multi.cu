@@ -76,7 +76,10 @@ struct MpcgCols {
   double* beta;
   double* rn;     // |r_c|: recurrence, or the FP64 residual after a recomputation
   int* live;      // 1 while column c iterates
+  double* ypart;  // [kind][column chunk][3]: per-chunk results of the reductions
+  unsigned int* yctr;  // [kind][column chunk]: arrival counters of the chunk reductions
 };
+constexpr int kMKinds = 5;
 
 __device__ __forceinline__ void mp_stop(MpcgState* st, int status) {
   st->status = status;
@@ -125,18 +128,68 @@ __device__ __forceinline__ void store_col_partials(const double (&v)[NQ], double
   }
 }
 
-// Fixed-order total of column c over the gx CTA partials.
-__device__ __forceinline__ double col_total(const double* bp, int gx, int k, int c) {
+// Two-level fixed-order reduction of the per-CTA column partials.  Level 1:
+// the last CTA of each column chunk (blockIdx.y) adds its 32 columns' partials
+// over the grid's CTAs (row lane r takes CTAs r, r + 8, ..., coalesced over the
+// columns; then the lanes in order) and applies the per-column logic in warp
+// 0 (lane = column); level 2: the last of those CTAs combines the chunks'
+// results (in chunk order) for the solve-wide decisions.
+
+// Level 1 entry: true in the CTA that completes this column chunk.
+__device__ __forceinline__ bool chunk_last(MpcgCols cols, int kind) {
+  return arrive_last_of(&cols.yctr[kind * gridDim.y + blockIdx.y], gridDim.x);
+}
+
+// Column totals of this chunk's 32 columns, valid in warp 0 (column
+// blockIdx.y * 32 + lane; zero for columns past k).  Whole CTA.
+template <int NQ>
+__device__ __forceinline__ void chunk_totals(const double* bp, int64_t qs, int k, double (&tot)[NQ]) {
+  __shared__ double sred[NQ][kRW][kCW];
+  const int tc = threadIdx.x % kCW, tr = threadIdx.x / kCW;
+  const int c = blockIdx.y * kCW + tc;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    double t = 0.0;
+    if (c < k)
+      for (unsigned int b = tr; b < gridDim.x; b += kRW) t += __ldcg(bp + q * qs + (int64_t)b * k + c);
+    sred[q][tr][tc] = t;
+  }
+  __syncthreads();
+  if (tr == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      double t = 0.0;
+#pragma unroll
+      for (int r = 0; r < kRW; ++r) t += sred[q][r][tc];
+      tot[q] = t;
+    }
+  }
+}
+
+// Level 2 entry (whole CTA, after warp 0 stored the chunk's results): true in
+// the CTA that completes the last chunk.
+__device__ __forceinline__ bool solve_last(MpcgState* st, int kind) {
+  return arrive_last_of(&st->counters[kind], gridDim.y);
+}
+
+// Sum of slot j of the chunks' results, in chunk order (one thread).
+__device__ __forceinline__ double chunks_sum(MpcgCols cols, int kind, int j) {
   double t = 0.0;
-  for (int b = 0; b < gx; ++b) t += __ldcg(bp + (int64_t)b * k + c);
+  for (unsigned int y = 0; y < gridDim.y; ++y) t += __ldcg(cols.ypart + ((int64_t)kind * gridDim.y + y) * 3 + j);
   return t;
+}
+
+__device__ __forceinline__ void put_chunk(MpcgCols cols, int kind, double a, double b, double c) {
+  double* d = cols.ypart + ((int64_t)kind * gridDim.y + blockIdx.y) * 3;
+  d[0] = a;
+  d[1] = b;
+  d[2] = c;
 }
 
 // X = 0 and R = B (unless warm start), |b_c| -> bnorm, |B|_F, tolerances.
 __global__ void __launch_bounds__(kMT)
     mp_init_kernel(const double* __restrict__ B, double* __restrict__ X, double* __restrict__ R,
                    int64_t n, int k, int has_x0, double* bp, MpcgState* st, MpcgCols cols) {
-  __shared__ double s_red[kMT / 32];
   const int c = blockIdx.y * kCW + threadIdx.x % kCW;
   double acc = 0.0;
   if (c < k) {
@@ -153,20 +206,25 @@ __global__ void __launch_bounds__(kMT)
   }
   const double v[1] = {acc};
   store_col_partials<1>(v, bp, 0, k);
-  if (!arrive_last_block(&st->counters[kMCtrInit])) return;
-  double fro = 0.0;
-  for (int cc = threadIdx.x; cc < k; cc += kMT) {
-    const double t = col_total(bp, gridDim.x, k, cc);
-    const double bn = sqrt(t);
-    cols.bnorm[cc] = bn;
-    cols.rn[cc] = bn;
-    cols.live[cc] = 1;
-    fro += t;
+  if (!chunk_last(cols, kMCtrInit)) return;
+  double tot[1];
+  chunk_totals<1>(bp, 0, k, tot);
+  if (threadIdx.x < kCW) {
+    const int cc = blockIdx.y * kCW + threadIdx.x;
+    double fro = 0.0;
+    if (cc < k) {
+      const double bn = sqrt(tot[0]);
+      cols.bnorm[cc] = bn;
+      cols.rn[cc] = bn;
+      cols.live[cc] = 1;
+      fro = tot[0];
+    }
+    fro = warp_sum(fro);
+    if (threadIdx.x == 0) put_chunk(cols, kMCtrInit, fro, 0.0, 0.0);
   }
-  double f[1] = {fro};
-  block_sum<kMT, 1>(f, s_red);
+  if (!solve_last(st, kMCtrInit)) return;
   if (threadIdx.x == 0) {
-    const double bn = sqrt(f[0]);
+    const double bn = sqrt(chunks_sum(cols, kMCtrInit, 0));
     st->bnorm = bn;
     st->tol_abs = st->tol * bn;
     st->rnorm = bn;
@@ -197,27 +255,32 @@ __global__ void __launch_bounds__(kMT)
   const int64_t qs = (int64_t)gridDim.x * k;
   const double v[3] = {d0, d1, d2};
   store_col_partials<3>(v, bp, qs, k);
-  if (!arrive_last_block(&st->counters[kMCtrMatvec])) return;
-  const double eps = st->eps;
-  bool nonfinite = false, breakdown = false;
-  for (int cc = threadIdx.x; cc < k; cc += kMT) {
-    if (!cols.live[cc]) {
-      cols.alpha[cc] = 0.0;
-      continue;
+  if (!chunk_last(cols, kMCtrMatvec)) return;
+  double tot[3];
+  chunk_totals<3>(bp, qs, k, tot);
+  if (threadIdx.x < kCW) {
+    const int cc = blockIdx.y * kCW + threadIdx.x;
+    bool nonfinite = false, breakdown = false;
+    if (cc < k) {
+      if (!cols.live[cc]) {
+        cols.alpha[cc] = 0.0;
+      } else {
+        const double pap = tot[0], pp = tot[1], aa = tot[2];
+        if (!isfinite(pap) || !isfinite(pp) || !isfinite(aa)) {
+          nonfinite = true;
+        } else if (pp > 0.0 && pap <= -st->eps * sqrt(pp) * sqrt(aa)) {
+          breakdown = true;  // non-positive curvature (laker/solvers.py:343-352)
+        }
+        cols.alpha[cc] = (pp > 0.0 && pap != 0.0) ? cols.rz[cc] / pap : 0.0;
+      }
     }
-    const double pap = col_total(bp, gridDim.x, k, cc);
-    const double pp = col_total(bp + qs, gridDim.x, k, cc);
-    const double aa = col_total(bp + 2 * qs, gridDim.x, k, cc);
-    if (!isfinite(pap) || !isfinite(pp) || !isfinite(aa)) {
-      nonfinite = true;
-    } else if (pp > 0.0 && pap <= -eps * sqrt(pp) * sqrt(aa)) {
-      breakdown = true;  // non-positive curvature (laker/solvers.py:343-352)
-    }
-    cols.alpha[cc] = (pp > 0.0 && pap != 0.0) ? cols.rz[cc] / pap : 0.0;
+    const bool nf = __any_sync(0xffffffffu, nonfinite), bd = __any_sync(0xffffffffu, breakdown);
+    if (threadIdx.x == 0) put_chunk(cols, kMCtrMatvec, nf ? 1.0 : 0.0, bd ? 1.0 : 0.0, 0.0);
   }
-  const int nf = __syncthreads_or(nonfinite ? 1 : 0);
-  const int bd = __syncthreads_or(breakdown ? 1 : 0);
+  if (!solve_last(st, kMCtrMatvec)) return;
   if (threadIdx.x == 0) {
+    const bool nf = chunks_sum(cols, kMCtrMatvec, 0) != 0.0;
+    const bool bd = chunks_sum(cols, kMCtrMatvec, 1) != 0.0;
     if (status_failed(dstatus)) mp_stop(st, *dstatus);
     else if (nf) mp_stop(st, LAKER_ERR_NONFINITE);
     else if (bd) mp_stop(st, LAKER_ERR_BREAKDOWN);
@@ -230,7 +293,6 @@ __global__ void __launch_bounds__(kMT)
                         double* __restrict__ X, double* __restrict__ R, int64_t n, int k, double* bp,
                         MpcgState* st, MpcgCols cols) {
   if (st->done) return;
-  __shared__ double s_red[kMT / 32];
   const int c = blockIdx.y * kCW + threadIdx.x % kCW;
   double acc = 0.0;
   if (c < k) {
@@ -246,22 +308,27 @@ __global__ void __launch_bounds__(kMT)
   }
   const double v[1] = {acc};
   store_col_partials<1>(v, bp, 0, k);
-  if (!arrive_last_block(&st->counters[kMCtrUpdate])) return;
-  const double tol = st->tol;
-  double fro = 0.0;
-  bool below = true;  // every live column's recurrence residual at its tolerance
-  for (int cc = threadIdx.x; cc < k; cc += kMT) {
-    const double t = col_total(bp, gridDim.x, k, cc);
-    const double rn = sqrt(t);
-    cols.rn[cc] = rn;
-    fro += t;
-    if (cols.live[cc] && !(rn <= tol * cols.bnorm[cc])) below = false;
+  if (!chunk_last(cols, kMCtrUpdate)) return;
+  double tot[1];
+  chunk_totals<1>(bp, 0, k, tot);
+  if (threadIdx.x < kCW) {
+    const int cc = blockIdx.y * kCW + threadIdx.x;
+    double fro = 0.0;
+    bool below = true;  // every live column's recurrence residual at its tolerance
+    if (cc < k) {
+      const double rn = sqrt(tot[0]);
+      cols.rn[cc] = rn;
+      fro = tot[0];
+      if (cols.live[cc] && !(rn <= st->tol * cols.bnorm[cc])) below = false;
+    }
+    fro = warp_sum(fro);
+    const bool all = __all_sync(0xffffffffu, below);
+    if (threadIdx.x == 0) put_chunk(cols, kMCtrUpdate, fro, all ? 0.0 : 1.0, 0.0);
   }
-  double f[1] = {fro};
-  block_sum<kMT, 1>(f, s_red);
-  const int all_below = __syncthreads_and(below ? 1 : 0);
+  if (!solve_last(st, kMCtrUpdate)) return;
   if (threadIdx.x == 0) {
-    const double rn = sqrt(f[0]);
+    const int all_below = chunks_sum(cols, kMCtrUpdate, 1) == 0.0 ? 1 : 0;
+    const double rn = sqrt(chunks_sum(cols, kMCtrUpdate, 0));
     st->rnorm = rn;
     st->iter += 1;
     if (rn > st->rmax) st->rmax = rn;
@@ -277,7 +344,6 @@ __global__ void __launch_bounds__(kMT)
     mp_after_residual_kernel(const double* __restrict__ R, int64_t n, int k, int init, double* bp,
                              MpcgState* st, MpcgCols cols) {
   if (st->done || (!init && !st->need_update)) return;
-  __shared__ double s_red[2 * (kMT / 32)];
   const int c = blockIdx.y * kCW + threadIdx.x % kCW;
   double acc = 0.0;
   if (c < k) {
@@ -289,31 +355,38 @@ __global__ void __launch_bounds__(kMT)
   }
   const double v[1] = {acc};
   store_col_partials<1>(v, bp, 0, k);
-  if (!arrive_last_block(&st->counters[kMCtrResid])) return;
-  const double tol = st->tol;
-  const bool freeze = st->column_stop && !init;
-  double fro = 0.0, live = 0.0;
-  bool nonfinite = false;
-  for (int cc = threadIdx.x; cc < k; cc += kMT) {
-    const double t = col_total(bp, gridDim.x, k, cc);
-    const double rn = sqrt(t);
-    cols.rn[cc] = rn;
-    fro += t;
-    if (!isfinite(rn)) nonfinite = true;
-    if (freeze && cols.live[cc] && rn <= tol * cols.bnorm[cc]) cols.live[cc] = 0;
-    live += cols.live[cc] ? 1.0 : 0.0;
+  if (!chunk_last(cols, kMCtrResid)) return;
+  double tot[1];
+  chunk_totals<1>(bp, 0, k, tot);
+  if (threadIdx.x < kCW) {
+    const int cc = blockIdx.y * kCW + threadIdx.x;
+    const bool freeze = st->column_stop && !init;
+    double fro = 0.0, live = 0.0;
+    bool nonfinite = false;
+    if (cc < k) {
+      const double rn = sqrt(tot[0]);
+      cols.rn[cc] = rn;
+      fro = tot[0];
+      if (!isfinite(rn)) nonfinite = true;
+      if (freeze && cols.live[cc] && rn <= st->tol * cols.bnorm[cc]) cols.live[cc] = 0;
+      live = cols.live[cc] ? 1.0 : 0.0;
+    }
+    fro = warp_sum(fro);
+    live = warp_sum(live);
+    const bool nf = __any_sync(0xffffffffu, nonfinite);
+    if (threadIdx.x == 0) put_chunk(cols, kMCtrResid, fro, live, nf ? 1.0 : 0.0);
   }
-  double f[2] = {fro, live};
-  block_sum<kMT, 2>(f, s_red);
-  const int nf = __syncthreads_or(nonfinite ? 1 : 0);
+  if (!solve_last(st, kMCtrResid)) return;
   if (threadIdx.x == 0) {
-    const double rn = sqrt(f[0]);
+    const bool nf = chunks_sum(cols, kMCtrResid, 2) != 0.0;
+    const double rn = sqrt(chunks_sum(cols, kMCtrResid, 0));
+    const double live_total = chunks_sum(cols, kMCtrResid, 1);
     st->rnorm = rn;
     st->true_rnorm = rn;
     st->rmax = rn;
     st->n_accurate += 1;
     st->need_update = 0;
-    st->n_live = (int)f[1];
+    st->n_live = (int)live_total;
     if (nf) {
       mp_stop(st, LAKER_ERR_NONFINITE);
     } else if (!init && (st->column_stop ? st->n_live == 0 : rn <= st->tol_abs)) {
@@ -350,21 +423,28 @@ __global__ void __launch_bounds__(kMT)
   }
   const double v[1] = {acc};
   store_col_partials<1>(v, bp, 0, k);
-  if (!arrive_last_block(&st->counters[kMCtrPrecond])) return;
-  bool nonfinite = false;
-  for (int cc = threadIdx.x; cc < k; cc += kMT) {
-    const double t = col_total(bp, gridDim.x, k, cc);
-    if (!isfinite(t)) nonfinite = true;
-    if (init) {
-      cols.beta[cc] = 0.0;
-    } else {
-      const double rz = cols.rz[cc];
-      cols.beta[cc] = (cols.live[cc] && rz != 0.0) ? t / rz : 0.0;
+  if (!chunk_last(cols, kMCtrPrecond)) return;
+  double tot[1];
+  chunk_totals<1>(bp, 0, k, tot);
+  if (threadIdx.x < kCW) {
+    const int cc = blockIdx.y * kCW + threadIdx.x;
+    bool nonfinite = false;
+    if (cc < k) {
+      const double t = tot[0];
+      if (!isfinite(t)) nonfinite = true;
+      if (init) {
+        cols.beta[cc] = 0.0;
+      } else {
+        const double rz = cols.rz[cc];
+        cols.beta[cc] = (cols.live[cc] && rz != 0.0) ? t / rz : 0.0;
+      }
+      cols.rz[cc] = t;
     }
-    cols.rz[cc] = t;
+    const bool nf = __any_sync(0xffffffffu, nonfinite);
+    if (threadIdx.x == 0) put_chunk(cols, kMCtrPrecond, nf ? 1.0 : 0.0, 0.0, 0.0);
   }
-  const int nf = __syncthreads_or(nonfinite ? 1 : 0);
-  if (threadIdx.x == 0 && nf) mp_stop(st, LAKER_ERR_NONFINITE);
+  if (!solve_last(st, kMCtrPrecond)) return;
+  if (threadIdx.x == 0 && chunks_sum(cols, kMCtrPrecond, 0) != 0.0) mp_stop(st, LAKER_ERR_NONFINITE);
 }
 
 // P = Z + P diag(beta) (P = Z when `init`); frozen columns get P_c = 0.
@@ -657,6 +737,8 @@ MpcgWs carve_multi(void* base, int64_t n, int k, int nr) {
   w.cols.beta = reinterpret_cast<double*>(take((size_t)k * sizeof(double)));
   w.cols.rn = reinterpret_cast<double*>(take((size_t)k * sizeof(double)));
   w.cols.live = reinterpret_cast<int*>(take((size_t)k * sizeof(int)));
+  w.cols.ypart = reinterpret_cast<double*>(take((size_t)kMKinds * g.gy * 3 * sizeof(double)));
+  w.cols.yctr = reinterpret_cast<unsigned int*>(take((size_t)kMKinds * g.gy * sizeof(unsigned int)));
   w.R = reinterpret_cast<double*>(take(nk * sizeof(double)));
   w.P = reinterpret_cast<float*>(take(nk * sizeof(float)));
   w.AP = reinterpret_cast<float*>(take(nk * sizeof(float)));
@@ -701,6 +783,8 @@ int pcg_solve_multi(const laker_operator* op, const laker_precond* pc, const dou
   h.active = 1;
   h.column_stop = prm->column_stop ? 1 : 0;
   cudaError_t e = cudaMemsetAsync(w.hdr, 0, kWsHeader, s);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(w.cols.yctr, 0, (size_t)kMKinds * g.gy * sizeof(unsigned int), s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(w.st, &h, sizeof(MpcgState), cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return fail_cuda(e);
 
