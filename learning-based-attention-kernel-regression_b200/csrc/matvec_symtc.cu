@@ -485,9 +485,12 @@ __global__ void __launch_bounds__(kTThreads, 1)
         if (nx.next<BATCHED>(sp, bm, n)) load_x(nx, xb_next, xa_next);
       }
       epi_bar_sync<kTEpi>();
-      double racc[kTRowTiles];
+      // a thread's share of a row sum (128 entries of the pair) in FP32, like
+      // the column sums (512 rows per pair), widened to FP64 once per pair:
+      // the per-chunk F2F + DADD chain cost 5 % of the kernel
+      float racc[kTRowTiles];
 #pragma unroll
-      for (int rt = 0; rt < kTRowTiles; ++rt) racc[rt] = 0.0;
+      for (int rt = 0; rt < kTRowTiles; ++rt) racc[rt] = 0.0f;
       for (int s = 0; s < nsl; ++s) {
         float xj[CW];
         {
@@ -517,7 +520,7 @@ __global__ void __launch_bounds__(kTThreads, 1)
             ra = __ffma2_rn(e, make_float2(xj[2 * u], xj[2 * u + 1]), ra);
             cacc[u] = __ffma2_rn(e, xr, cacc[u]);
           }
-          racc[rt] += (double)(ra.x + ra.y);
+          racc[rt] += ra.x + ra.y;
         };
 #pragma unroll
         for (int hp = 0; hp < kTRowTiles / UT; ++hp, ++g) {
@@ -560,7 +563,7 @@ __global__ void __launch_bounds__(kTThreads, 1)
           sCol[q * kTB + s * kTSlabN + cg * CW + (CW == 32 ? lane : (lane >> 1))] = 0.0f;
       }
 #pragma unroll
-      for (int rt = 0; rt < kTRowTiles; ++rt) sRow[cg * kTB + rt * 128 + q * 32 + lane] = racc[rt];
+      for (int rt = 0; rt < kTRowTiles; ++rt) sRow[cg * kTB + rt * 128 + q * 32 + lane] = (double)racc[rt];
       epi_bar_sync<kTEpi>();
       for (int j = tid; j < kTB; j += kTEpi) {
         double r = sRow[j];
