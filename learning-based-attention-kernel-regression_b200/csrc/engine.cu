@@ -167,6 +167,19 @@ __device__ void w_multiply(const EngineDev& ed, const BlockCtx& c, double* s_u) 
     const float* up = ed.upart + c.b0 * ed.ustride + col;
     double u0 = 0.0, u1 = 0.0, u2 = 0.0, u3 = 0.0;
     unsigned b = 0;
+    // 16 loads issued before their adds (same partial sums, same order)
+    for (; b + 16 <= c.nblk; b += 16) {
+      float t[16];
+#pragma unroll
+      for (int e = 0; e < 16; ++e) t[e] = __ldcg(up + (int64_t)(b + e) * ed.ustride);
+#pragma unroll
+      for (int e = 0; e < 16; e += 4) {
+        u0 += (double)t[e];
+        u1 += (double)t[e + 1];
+        u2 += (double)t[e + 2];
+        u3 += (double)t[e + 3];
+      }
+    }
     for (; b + 4 <= c.nblk; b += 4) {
       u0 += (double)__ldcg(up + (int64_t)b * ed.ustride);
       u1 += (double)__ldcg(up + (int64_t)(b + 1) * ed.ustride);
@@ -183,6 +196,19 @@ __device__ void w_multiply(const EngineDev& ed, const BlockCtx& c, double* s_u) 
     if (col < nr) {
       const float* wc = W + col;
       int cc = 0;
+      // 16 loads of W issued before their FMAs (same partial sums, same order)
+      for (; cc + 16 <= nr; cc += 16) {
+        float t[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) t[e] = __ldg(wc + (int64_t)(cc + e) * nr);
+#pragma unroll
+        for (int e = 0; e < 16; e += 4) {
+          a0 = fma((double)t[e], s_u[cc + e], a0);
+          a1 = fma((double)t[e + 1], s_u[cc + e + 1], a1);
+          a2 = fma((double)t[e + 2], s_u[cc + e + 2], a2);
+          a3 = fma((double)t[e + 3], s_u[cc + e + 3], a3);
+        }
+      }
       for (; cc + 4 <= nr; cc += 4) {
         a0 = fma((double)wc[(int64_t)cc * nr], s_u[cc], a0);
         a1 = fma((double)wc[(int64_t)(cc + 1) * nr], s_u[cc + 1], a1);

@@ -110,15 +110,32 @@ __global__ void __launch_bounds__(T)
   }
   if (!arrive_last_block(counter)) return;
   const int nr = pc.nr;
+  // both sums in one fixed order, with 16 loads issued ahead of their adds
   for (int c = threadIdx.x; c < nr; c += T) {
     double u = 0.0;
-    for (unsigned int b = 0; b < gridDim.x; ++b) u += __ldcg(upart + (int64_t)b * pc.ldq + c);
+    unsigned int b = 0;
+    for (; b + 16 <= gridDim.x; b += 16) {
+      double t[16];
+#pragma unroll
+      for (int e = 0; e < 16; ++e) t[e] = __ldcg(upart + (int64_t)(b + e) * pc.ldq + c);
+#pragma unroll
+      for (int e = 0; e < 16; ++e) u += t[e];
+    }
+    for (; b < gridDim.x; ++b) u += __ldcg(upart + (int64_t)b * pc.ldq + c);
     s_u[c] = u;
   }
   __syncthreads();
   for (int c = threadIdx.x; c < nr; c += T) {
     double acc2 = 0.0;
-    for (int cc = 0; cc < nr; ++cc) acc2 = fma((double)pc.W[(int64_t)cc * nr + c], s_u[cc], acc2);
+    int cc = 0;
+    for (; cc + 16 <= nr; cc += 16) {
+      float t[16];
+#pragma unroll
+      for (int e = 0; e < 16; ++e) t[e] = __ldg(pc.W + (int64_t)(cc + e) * nr + c);
+#pragma unroll
+      for (int e = 0; e < 16; ++e) acc2 = fma((double)t[e], s_u[cc + e], acc2);
+    }
+    for (; cc < nr; ++cc) acc2 = fma((double)pc.W[(int64_t)cc * nr + c], s_u[cc], acc2);
     v[c] = acc2;
   }
 }

@@ -194,6 +194,25 @@ __device__ __forceinline__ void tmem_st_wait() {
   asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
+// try_wait that may suspend the thread until the phase completes or about
+// `hint_ns` have passed (instead of returning at once), so a waiting warp
+// stops taking issue slots from the warps doing the work.  The pipeline waits
+// use 20 us (measured 1-2 % faster than polling for k1t and the flash
+// multi-RHS kernel; each wait still checks the abort flag and its time limit
+// after every suspension).
+constexpr uint32_t kWaitHintNs = 20000;
+__device__ __forceinline__ bool mbar_try_wait_hint(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
@@ -212,11 +231,9 @@ __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, in
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_timer_ns();
   for (uint32_t it = 0; it < (1u << 30); ++it) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if ((it & 63u) == 0) {
-      if (*abort) return false;
-      if (global_timer_ns() - t0 >= limit) break;
-    }
+    if (mbar_try_wait_hint(bar, parity, kWaitHintNs)) return true;
+    if (*abort) return false;
+    if (global_timer_ns() - t0 >= limit) break;
   }
   record_status(status, LAKER_ERR_TIMEOUT);
   *abort = 1;
