@@ -24,6 +24,7 @@ __global__ void __launch_bounds__(T, 2)
   constexpr int TILE = TC * DP;
   __shared__ __align__(128) double sE[2][TILE];
   __shared__ __align__(16) double sX[2][TC];
+  __shared__ double sExp[64];
   __shared__ __align__(8) uint64_t bar[2];
 
   const int tid = threadIdx.x;
@@ -48,6 +49,7 @@ __global__ void __launch_bounds__(T, 2)
     mbar_init(&bar[1], 1);
     mbar_fence_init();
   }
+  exp_table_to_shared(sExp, tid, T);
   __syncthreads();
 
   auto issue = [&](int t, int b) {
@@ -98,7 +100,7 @@ __global__ void __launch_bounds__(T, 2)
 #pragma unroll
         for (int k = 1; k < DP; ++k) s = fma(ev[r][k], c[k], s);
         if (CLAMP) s = fmin(s, kClamp64);
-        acc[r] = fma(exp(s), xj, acc[r]);
+        acc[r] = fma(exp_tab(s, sExp), xj, acc[r]);
       }
     }
     __syncthreads();

@@ -354,6 +354,7 @@ __global__ void __launch_bounds__(T, 1)
   __shared__ __align__(128) double sE[2][TILE];
   __shared__ __align__(16) double sX[2][TC];
   __shared__ double sCol[NW][TC];
+  __shared__ double sExp[64];
   __shared__ __align__(8) uint64_t bar[2];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -390,6 +391,7 @@ __global__ void __launch_bounds__(T, 1)
     mbar_init(&bar[1], 1);
     mbar_fence_init();
   }
+  exp_table_to_shared(sExp, tid, T);
   __syncthreads();
 
   auto col0_of = [&](const SymCursor& s) -> int64_t { return s.seg + s.b * B + (int64_t)s.t * TC; };
@@ -429,7 +431,7 @@ __global__ void __launch_bounds__(T, 1)
 #pragma unroll
     for (int k = 1; k < DP; ++k) s = fma(ev[r][k], cp[k], s);
     if (CLAMP) s = fmin(s, kClamp64);
-    return exp(s);
+    return exp_tab(s, sExp);
   };
 
   load_rows(cu);
