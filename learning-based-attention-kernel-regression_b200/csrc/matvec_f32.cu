@@ -265,7 +265,9 @@ __global__ void __launch_bounds__((kMBM / 4) * (BN / 4))
   __shared__ __align__(16) Real sCol[kMBK][DP + 1];
   __shared__ __align__(16) Real sP[kMBK][kMBM];
   __shared__ __align__(16) Real sX[kMBK][BN];
+  __shared__ double sExp[64];
   const int tid = threadIdx.x;
+  if constexpr (sizeof(Real) == 8) exp_table_to_shared(sExp, tid, T);
   const int tx = tid % (BN / 4), ty = tid / (BN / 4);
   const int64_t i0 = (int64_t)blockIdx.x * kMBM;
   const int64_t c0 = (int64_t)blockIdx.y * BN;
@@ -286,27 +288,65 @@ __global__ void __launch_bounds__((kMBM / 4) * (BN / 4))
       rv[kk] = v;
     }
   }
+  // FP32: FP32 microtile sums flushed to FP64 every 8 steps; FP64: the
+  // microtile accumulates in FP64 directly
+  constexpr bool kF64 = sizeof(Real) == 8;
   Real acc[4][4];
-  double acc64[4][4];
+  double acc64[kF64 ? 1 : 4][kF64 ? 1 : 4];
 #pragma unroll
   for (int u = 0; u < 4; ++u)
 #pragma unroll
-    for (int v = 0; v < 4; ++v) acc[u][v] = Real(0), acc64[u][v] = 0.0;
+    for (int v = 0; v < 4; ++v) acc[u][v] = Real(0);
+  if constexpr (!kF64) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) acc64[u][v] = 0.0;
+  }
 
-  const int nsteps = (int)ceil_div(n, kMBK);
-  for (int st = 0; st < nsteps; ++st) {
+  // The next step's column embeddings and X tile are loaded into registers
+  // while this step computes, and stored into shared memory after it.
+  constexpr int kPC = (kMBK * DP + T - 1) / T, kPX = (kMBK * BN) / T;
+  static_assert((kMBK * BN) % T == 0, "X tile / thread mapping");
+  Real pc[kPC], px[kPX];
+  auto fetch = [&](int st) {
     const int64_t j0 = (int64_t)st * kMBK;
-    for (int o = tid; o < kMBK * DP; o += T) {
+#pragma unroll
+    for (int t = 0; t < kPC; ++t) {
+      const int o = tid + t * T;
       const int jj = o / DP, kk = o - jj * DP;
       const int64_t j = j0 + jj;
-      sCol[jj][kk] = (j < n) ? emb(cols, col_layout_pairs, j, kk) : Real(0);
+      pc[t] = (o < kMBK * DP && j < n) ? emb(cols, col_layout_pairs, j, kk) : Real(0);
     }
-    for (int o = tid; o < kMBK * BN; o += T) {
+#pragma unroll
+    for (int t = 0; t < kPX; ++t) {
+      const int o = tid + t * T;
       const int jj = o / BN, cc = o - jj * BN;
       const int64_t j = j0 + jj, c = c0 + cc;
-      sX[jj][cc] = (j < n && c < k) ? X[j * ldx + c] : Real(0);
+      px[t] = (j < n && c < k) ? X[j * ldx + c] : Real(0);
     }
+  };
+  auto store = [&]() {
+#pragma unroll
+    for (int t = 0; t < kPC; ++t) {
+      const int o = tid + t * T;
+      if (o < kMBK * DP) sCol[o / DP][o % DP] = pc[t];
+    }
+#pragma unroll
+    for (int t = 0; t < kPX; ++t) {
+      const int o = tid + t * T;
+      sX[o / BN][o % BN] = px[t];
+    }
+  };
+
+  const int nsteps = (int)ceil_div(n, kMBK);
+  if (nsteps > 0) {
+    fetch(0);
+    store();
+  }
+  for (int st = 0; st < nsteps; ++st) {
     __syncthreads();
+    if (st + 1 < nsteps) fetch(st + 1);
 #pragma unroll
     for (int q = 0; q < (kMBM * kMBK) / T; ++q) {
       const int jj = tid / kMBM + (T / kMBM) * q;
@@ -319,7 +359,7 @@ __global__ void __launch_bounds__((kMBM / 4) * (BN / 4))
         e = ex2_approx(s);
       } else {
         if (CLAMP) s = fmin(s, kClamp64);
-        e = exp(s);
+        e = exp_tab(s, sExp);
       }
       sP[jj][a] = e;
     }
@@ -334,13 +374,16 @@ __global__ void __launch_bounds__((kMBM / 4) * (BN / 4))
 #pragma unroll
         for (int v = 0; v < 4; ++v) acc[u][v] = fma(pa[u], xb[v], acc[u][v]);
     }
-    if ((st & 7) == 7 || st == nsteps - 1) {
+    if constexpr (!kF64) {
+      if ((st & 7) == 7 || st == nsteps - 1) {
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
+        for (int u = 0; u < 4; ++u)
 #pragma unroll
-        for (int v = 0; v < 4; ++v) acc64[u][v] += (double)acc[u][v], acc[u][v] = Real(0);
+          for (int v = 0; v < 4; ++v) acc64[u][v] += (double)acc[u][v], acc[u][v] = Real(0);
+      }
     }
     __syncthreads();
+    if (st + 1 < nsteps) store();
   }
 
   const bool square = (m == n);
@@ -352,7 +395,9 @@ __global__ void __launch_bounds__((kMBM / 4) * (BN / 4))
     for (int v = 0; v < 4; ++v) {
       const int64_t c = c0 + tx * 4 + v;
       if (c >= k) continue;
-      double y = acc64[u][v];
+      double y;
+      if constexpr (kF64) y = acc[u][v];
+      else y = acc64[u][v];
       if (square) y += (double)lam * (double)X[i * ldx + c];
       if (RESIDUAL) y = (double)B[i * ldb + c] - y;
       Y[i * ldy + c] = (Real)y;
