@@ -11,8 +11,8 @@ classes (tests/golden/make_golden.py) in float64 on the CPU:
 * fit_n2000: the config-1 fit of LAKERRegressor (laker/models.py:392-537):
   embeddings, alpha, 2000 predictions and 64 predictive variances.
 
-The GPU path must reproduce them within the tolerances the north star states:
-true relative residual <= 1e-6 and prediction error <= 1e-5 against float64.
+The GPU path must reproduce them within the tolerances the solve path is held
+to: true relative residual <= 1e-6 and prediction error <= 1e-5 against float64.
 """
 
 import numpy as np
