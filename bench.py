@@ -510,7 +510,8 @@ def roofline_block(kernel_id, work, k1_avg_ms, achieved, exps_per_s, peaks, traf
 def kernel_only(args) -> None:
     """One fused matvec alone on the bench embeddings (a clean ncu target):
     the FP32 single-RHS operator, or with --rhs k > 1 the tensor-core
-    multi-RHS operator."""
+    multi-RHS operator; with --kernel-precision f64 the FP64 (residual)
+    operator instead."""
     import laker_b200 as L
 
     dev = torch.device("cuda", 0)
@@ -519,21 +520,27 @@ def kernel_only(args) -> None:
     with torch.no_grad():
         E = emb(x.to(dev))
     op = L.AttentionKernelOperator(E, lambda_reg=LAMBDA)
-    v = torch.randn(args.n, device=dev) if args.rhs <= 1 else torch.randn(args.n, args.rhs, device=dev)
+    f64 = args.kernel_precision == "f64"
+    dt = torch.float64 if f64 else torch.float32
+    v = (torch.randn(args.n, device=dev, dtype=dt) if args.rhs <= 1
+         else torch.randn(args.n, args.rhs, device=dev, dtype=dt))
+    apply = op.matvec_f64 if f64 else op.matvec
     for _ in range(args.warmup):
-        op.matvec(v)
+        apply(v)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(args.steps):
-        op.matvec(v)
+        apply(v)
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / max(args.steps, 1)
     k = max(args.rhs, 1)
-    out = {"kernel": "fp32 fused matvec" if k == 1 else "tensor-core multi-RHS matvec", "n": args.n,
+    name = ("fp64 fused matvec" if k == 1 else "fp64 multi-RHS matvec") if f64 else \
+        ("fp32 fused matvec" if k == 1 else "tensor-core multi-RHS matvec")
+    out = {"kernel": name, "n": args.n,
            "rhs": k, "ms": ms, "entries_per_s": args.n * args.n / (ms * 1e-3)}
-    if k > 1:
+    if k > 1 and not f64:
         out["tf32_tflops_3_products"] = 3 * 2.0 * args.n * args.n * k / (ms * 1e-3) / 1e12
     print(json.dumps(out))
 
@@ -1128,6 +1135,8 @@ def main() -> None:
                     "fit+predict; variance: n=20k x 512 queries; batch: 1024 instances; serve: "
                     "Poisson request trace; sharded: one n=100k solve row-sharded over the GPUs")
     ap.add_argument("--rhs", type=int, default=1, help="--kernel-only: right-hand sides")
+    ap.add_argument("--kernel-precision", choices=("f32", "f64"), default="f32",
+                    help="--kernel-only: the FP32 operator or the FP64 (residual) operator")
     ap.add_argument("--count", type=int, default=1024, help="batch: instances")
     ap.add_argument("--plain-subset", type=int, default=64, help="batch: single-path sample")
     ap.add_argument("--requests", type=int, default=120, help="serve: requests per rate")
