@@ -492,21 +492,33 @@ __global__ void __launch_bounds__(kMT)
   const int64_t i_end = min(n, i_begin + chunk_rows);
   float acc[4][4] = {};
   const int rr = tid / 16, cg = tid % 16;
-  for (int64_t i = i_begin; i < i_end; i += kGK) {
+  // the next K step's tiles are loaded into registers while this one computes
+  float4 qn;
+  float rn[4];
+  auto fetch = [&](int64_t i) {
     const int64_t ii = i + rr;
     const bool row_ok = ii < i_end;
-    {
-      const int j = j0 + cg * 4;
-      float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (row_ok && j < nq) q = *reinterpret_cast<const float4*>(Q + ii * ldq + j);
-      *reinterpret_cast<float4*>(&Qs[rr][cg * 4]) = q;
-    }
+    const int j = j0 + cg * 4;
+    qn = (row_ok && j < nq) ? *reinterpret_cast<const float4*>(Q + ii * ldq + j)
+                            : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
       const int c = c0 + cg * 4 + v;
-      Rs[rr][cg * 4 + v] = (row_ok && c < k) ? (float)R[ii * k + c] : 0.0f;
+      rn[v] = (row_ok && c < k) ? (float)R[ii * k + c] : 0.0f;
     }
+  };
+  auto store = [&]() {
+    *reinterpret_cast<float4*>(&Qs[rr][cg * 4]) = qn;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) Rs[rr][cg * 4 + v] = rn[v];
+  };
+  if (i_begin < i_end) {
+    fetch(i_begin);
+    store();
+  }
+  for (int64_t i = i_begin; i < i_end; i += kGK) {
     __syncthreads();
+    if (i + kGK < i_end) fetch(i + kGK);
 #pragma unroll
     for (int kk = 0; kk < kGK; ++kk) {
       const float4 a = *reinterpret_cast<const float4*>(&Qs[kk][ty * 4]);
@@ -518,6 +530,7 @@ __global__ void __launch_bounds__(kMT)
         for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(av[u], bv[v], acc[u][v]);
     }
     __syncthreads();
+    if (i + kGK < i_end) store();
   }
 #pragma unroll
   for (int u = 0; u < 4; ++u) {
@@ -591,28 +604,38 @@ __global__ void __launch_bounds__(kMT)
   const int64_t i0 = (int64_t)blockIdx.x * kGT;
   const int c0 = blockIdx.y * kGT;
   float acc[4][4] = {};
-  for (int j = 0; j < nr; j += kGK) {
-    {
-      const int ii = tid / 4, cg = tid % 4;  // 64 rows x 4 groups of 4 columns
-      const int64_t i = i0 + ii;
-      const int jc = j + cg * 4;
-      float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (i < n && jc < nq) q = *reinterpret_cast<const float4*>(Q + i * ldq + jc);
-      Qs[cg * 4 + 0][ii] = q.x;
-      Qs[cg * 4 + 1][ii] = q.y;
-      Qs[cg * 4 + 2][ii] = q.z;
-      Qs[cg * 4 + 3][ii] = q.w;
-    }
-    {
-      const int rr = tid / 16, cg = tid % 16;
-      const int jr = j + rr;
+  // the next K step's tiles are loaded into registers while this one computes
+  const int qi = tid / 4, qg = tid % 4;  // Q tile: 64 rows x 4 groups of 4 columns
+  const int vr = tid / 16, vg = tid % 16;  // V tile: 16 rows x 16 groups of 4 columns
+  float4 qn;
+  float vn[4];
+  auto fetch = [&](int j) {
+    const int64_t i = i0 + qi;
+    const int jc = j + qg * 4;
+    qn = (i < n && jc < nq) ? *reinterpret_cast<const float4*>(Q + i * ldq + jc)
+                            : make_float4(0.f, 0.f, 0.f, 0.f);
+    const int jr = j + vr;
 #pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        const int c = c0 + cg * 4 + v;
-        Vs[rr][cg * 4 + v] = (jr < nr && c < k) ? (float)V[(int64_t)jr * k + c] : 0.0f;
-      }
+    for (int v = 0; v < 4; ++v) {
+      const int c = c0 + vg * 4 + v;
+      vn[v] = (jr < nr && c < k) ? (float)V[(int64_t)jr * k + c] : 0.0f;
     }
+  };
+  auto store = [&]() {
+    Qs[qg * 4 + 0][qi] = qn.x;
+    Qs[qg * 4 + 1][qi] = qn.y;
+    Qs[qg * 4 + 2][qi] = qn.z;
+    Qs[qg * 4 + 3][qi] = qn.w;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) Vs[vr][vg * 4 + v] = vn[v];
+  };
+  if (nr > 0) {
+    fetch(0);
+    store();
+  }
+  for (int j = 0; j < nr; j += kGK) {
     __syncthreads();
+    if (j + kGK < nr) fetch(j + kGK);
 #pragma unroll
     for (int kk = 0; kk < kGK; ++kk) {
       const float4 a = *reinterpret_cast<const float4*>(&Qs[kk][ty * 4]);
@@ -624,6 +647,7 @@ __global__ void __launch_bounds__(kMT)
         for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(av[u], bv[v], acc[u][v]);
     }
     __syncthreads();
+    if (j + kGK < nr) store();
   }
 #pragma unroll
   for (int u = 0; u < 4; ++u) {
