@@ -299,7 +299,9 @@ __global__ void __launch_bounds__(kFThreads, 1)
 #pragma unroll
           for (int u = 0; u < 16; ++u) {
             const float p = ex2_approx(v[16 * h + u]);
-            hi[u] = to_tf32(p);
+            // P_hi by truncation (an AND instead of a conversion), P_lo the
+            // exact remainder rounded to TF32: |error| <= 2^-22 |p|
+            hi[u] = __float_as_uint(p) & 0xffffe000u;
             lo[u] = to_tf32(p - __uint_as_float(hi[u]));
           }
           tmem_st16(ts + (uint32_t)(16 * h), hi);
