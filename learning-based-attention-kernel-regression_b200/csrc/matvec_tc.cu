@@ -305,10 +305,12 @@ __global__ void __launch_bounds__(kTcThreadsWs, 1)
             p[2 * h + 1] = row_ok ? ex2_approx(sacc.y) : 0.0f;
           }
           uint4 hi, lo;
-          hi.x = to_tf32(p[0]);
-          hi.y = to_tf32(p[1]);
-          hi.z = to_tf32(p[2]);
-          hi.w = to_tf32(p[3]);
+          // P_hi by truncation (an AND), P_lo the exact remainder rounded to
+          // TF32: |error| <= 2^-22 |p|
+          hi.x = __float_as_uint(p[0]) & 0xffffe000u;
+          hi.y = __float_as_uint(p[1]) & 0xffffe000u;
+          hi.z = __float_as_uint(p[2]) & 0xffffe000u;
+          hi.w = __float_as_uint(p[3]) & 0xffffe000u;
           lo.x = to_tf32(p[0] - __uint_as_float(hi.x));
           lo.y = to_tf32(p[1] - __uint_as_float(hi.y));
           lo.z = to_tf32(p[2] - __uint_as_float(hi.z));
@@ -633,7 +635,7 @@ __global__ void __launch_bounds__(kK2tThreads, 1)
           for (int u = 0; u < 4; ++u) {
             const float sv = v[4 * c4 + u];
             const float p = ex2_approx(CLAMP ? fminf(sv, kClampLog2) : sv);
-            ph[u] = to_tf32(p);
+            ph[u] = __float_as_uint(p) & 0xffffe000u;  // truncation, as in k2_tc_matvec
             pl[u] = to_tf32(p - __uint_as_float(ph[u]));
           }
           const uint32_t off = TileCfg<TK>::offset((uint32_t)row, (uint32_t)(h * 16 + 4 * c4));
