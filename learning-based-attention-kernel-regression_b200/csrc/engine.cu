@@ -625,7 +625,7 @@ EngineLayout engine_layout(const laker_engine_config& cfg) {
   L.o_row64 = take(PP * 8);
   L.o_col64 = take(PP * 8);
   L.tc = k1t_enabled(cfg.d);
-  L.fmt = k1t_format(cfg.clamp);
+  L.fmt = k1t_format(cfg.clamp, cfg.d);
   if (L.tc) L.o_img = take(k1t_image_bytes(L.cap_points));
   L.bytes = o;
   return L;

@@ -612,7 +612,7 @@ extern "C" int laker_attn_matvec_f32(const float* rows32, int64_t m, const float
     float* colpart = sym_colpart_ptr<float>(wbase, sp);
     if (tc) {
       uint8_t* img = reinterpret_cast<uint8_t*>(wbase) + round_up((int64_t)sym_partial_bytes<float>(sp), 1024);
-      const int fmt = k1t_format(clamp);
+      const int fmt = k1t_format(clamp, d);
       e = launch_k1t_pack(cols32, n, d, img, sp.nb * sym_block_points(), s, fmt);
       if (e == cudaSuccess)
         e = launch_k1t(img, n, clamp, X, rowpart, colpart, sp, &hdr->status, nullptr, s, fmt);

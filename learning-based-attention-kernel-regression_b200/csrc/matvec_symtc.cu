@@ -90,7 +90,9 @@ template <int UT, int FMT>
 struct K1tCfg {
   static_assert(UT == 2 || UT == 4, "row tiles per unit");
   static constexpr int kBufs = 8 / UT;
-  static constexpr uint32_t kHalf = FMT == kK1tF16 ? kTHalf16 : kTHalf;  // one side of a block
+  static constexpr uint32_t kHalf = FMT == kK1tF16 ? kTHalf16
+                                    : FMT == kK1tF16x2 ? 2 * kTVar16
+                                                       : kTHalf;  // one side of a block
   // mbarrier slots: row operands full / empty, column stages full [2] /
   // empty [2], TMEM buffers full [kBufs] / empty [kBufs], MMA drain
   static constexpr int kBarAFull = 0, kBarAEmpty = 1, kBarBFull = 2, kBarBEmpty = 4,
@@ -154,6 +156,58 @@ __global__ void k1t_pack16_kernel(const float* __restrict__ packed32, int DP, in
       q.z = (uint32_t)h[vv][4] | ((uint32_t)h[vv][5] << 16);
       q.w = (uint32_t)h[vv][6] | ((uint32_t)h[vv][7] << 16);
       *reinterpret_cast<uint4*>(base + vv * kTVar16) = q;
+    }
+  }
+}
+
+// Two-MMA FP16 image (DP <= 10) of `rows` points: one thread per point.
+// Per side two variants of 16 FP16: V0 = [H_0..H_DP-1 | Hs_0..Hs_P-1] and
+// V1 = [Hs_P..Hs_DP-1 | L_0..L_DP-1 | 0 ...] for the row side (scaled by
+// log2 e), W0 = [H' | L'_0..L'_P-1] and W1 = [L'_P..L'_DP-1 | Hs' | 0 ...]
+// for the column side, with P = min(16 - DP, DP): V0 W0 + V1 W1 =
+// H H' + Hs L' + L Hs', the three products of the split-FP16 format.
+__global__ void k1t_pack16x2_kernel(const float* __restrict__ packed32, int DP, int64_t npts,
+                                    int64_t rows, uint8_t* __restrict__ img) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    uint16_t hr[3][16], hc[3][16];  // [H, L, Hs] of the row and column sides
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const float v = (r < npts && k < DP) ? packed32[(r >> 1) * (2 * DP) + 2 * k + (r & 1)] : 0.0f;
+      split_f16(v * kLog2e, hr[0][k], hr[1][k], hr[2][k]);
+      split_f16(v, hc[0][k], hc[1][k], hc[2][k]);
+    }
+    const int P = (16 - DP) < DP ? 16 - DP : DP;
+    uint16_t out[4][16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      // V0 / W0: H, then the first P correction terms in H's padding
+      const bool lead = k < DP;
+      const int kp = k - DP;  // index into the padding
+      out[0][k] = lead ? hr[0][k] : (kp < P ? hr[2][kp] : 0);
+      out[2][k] = lead ? hc[0][k] : (kp < P ? hc[1][kp] : 0);
+      // V1 / W1: the remaining DP - P correction terms, then the second product
+      const int rest = DP - P;
+      const int k2 = k - rest;
+      out[1][k] = k < rest ? hr[2][P + k] : (k2 < DP ? hr[1][k2] : 0);
+      out[3][k] = k < rest ? hc[1][P + k] : (k2 < DP ? hc[2][k2] : 0);
+    }
+    const int64_t blk = r / kTB;
+    const uint32_t rr = (uint32_t)(r - blk * kTB);
+    uint8_t* base = img + blk * (int64_t)kTImgBlock;
+#pragma unroll
+    for (int vv = 0; vv < 4; ++vv) {
+      // variants 0, 1 on the row side; 2, 3 start the column side (2 * kTVar16)
+      uint8_t* vb = base + vv * kTVar16;
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        uint4 q;
+        q.x = (uint32_t)out[vv][8 * c + 0] | ((uint32_t)out[vv][8 * c + 1] << 16);
+        q.y = (uint32_t)out[vv][8 * c + 2] | ((uint32_t)out[vv][8 * c + 3] << 16);
+        q.z = (uint32_t)out[vv][8 * c + 4] | ((uint32_t)out[vv][8 * c + 5] << 16);
+        q.w = (uint32_t)out[vv][8 * c + 6] | ((uint32_t)out[vv][8 * c + 7] << 16);
+        *reinterpret_cast<uint4*>(vb + k1t16_offset(rr, 8u * c)) = q;
+      }
     }
   }
 }
@@ -273,7 +327,8 @@ __global__ void __launch_bounds__(kTThreads, 1)
                float* __restrict__ colpart, double* __restrict__ rowpart, SymPlan sp, BatchMap bm,
                int* status, const int* gate) {
   using Cfg = K1tCfg<UT, FMT>;
-  constexpr bool F16 = FMT == kK1tF16;
+  constexpr bool F16 = FMT != kK1tTf32;   // both FP16 formats
+  constexpr bool F16X2 = FMT == kK1tF16x2;  // the two-MMA FP16 format
   constexpr int CW = kTCW;
   constexpr int kTBufs = Cfg::kBufs;
   if (gate && *gate == 0) return;
@@ -421,7 +476,11 @@ __global__ void __launch_bounds__(kTThreads, 1)
             const int rt = UT * hp + r2;
             const uint32_t d = tmem_base + (uint32_t)(buf * (UT * kTSlabN) + r2 * kTSlabN);
             const uint64_t ahi = a_hi0 + (uint64_t)rt * kRowTileStep, alo = ahi + kLoStep;
-            if constexpr (F16) {
+            if constexpr (F16X2) {
+              // V0 W0 + V1 W1 = H H' + Hs L' + L Hs'
+              mma_f16(d, ahi, bhi, idesc, 0u);
+              mma_f16(d, alo, blo, idesc, 1u);
+            } else if constexpr (F16) {
               // variants H, L, Hs: H H' + Hs L' + L Hs'
               mma_f16(d, ahi, bhi, idesc, 0u);
               mma_f16(d, ahi + 2 * kLoStep, blo, idesc, 1u);
@@ -626,9 +685,12 @@ template <bool CLAMP, bool BATCHED>
 cudaError_t launch_k1t_ut(const uint8_t* img, int64_t n, const float* x, double* rowpart,
                           float* colpart, const SymPlan& sp, const BatchMap& bm, int* status,
                           const int* gate, cudaStream_t s, int fmt) {
-  if (fmt == kK1tF16) {
+  if (fmt == kK1tF16 || fmt == kK1tF16x2) {
     // FP16 operands only for unclamped operators (|e_k| < 9: no overflow)
     if (CLAMP) return cudaErrorInvalidValue;
+    if (fmt == kK1tF16x2)
+      return launch_k1t_t<4, kK1tF16x2, false, BATCHED>(img, n, x, rowpart, colpart, sp, bm,
+                                                         status, gate, s);
     return launch_k1t_t<4, kK1tF16, false, BATCHED>(img, n, x, rowpart, colpart, sp, bm, status,
                                                      gate, s);
   }
@@ -648,8 +710,9 @@ bool k1t_enabled(int d) {
   return v == 1 && d >= 1 && d <= 16;
 }
 
-int k1t_format(int clamp) {
-  return (!clamp && variant_get(LAKER_VARIANT_K1T_LOGITS) == 1) ? kK1tF16 : kK1tTf32;
+int k1t_format(int clamp, int d) {
+  if (clamp || variant_get(LAKER_VARIANT_K1T_LOGITS) != 1) return kK1tTf32;
+  return padded_dim(d) <= 10 ? kK1tF16x2 : kK1tF16;
 }
 
 size_t k1t_image_bytes(int64_t points) {
@@ -677,13 +740,16 @@ SymPlan k1t_plan(int64_t n) {
 
 cudaError_t launch_k1t_pack(const float* packed32, int64_t npts, int d, uint8_t* img, int64_t rows,
                             cudaStream_t s, int fmt) {
-  if (rows % kTB != 0 || d < 1 || d > 16 || (fmt != kK1tTf32 && fmt != kK1tF16))
+  if (rows % kTB != 0 || d < 1 || d > 16 || (fmt != kK1tTf32 && fmt != kK1tF16 && fmt != kK1tF16x2))
     return cudaErrorInvalidValue;
-  const int per_point = fmt == kK1tF16 ? 2 : 4;  // threads per point
+  if (fmt == kK1tF16x2 && padded_dim(d) > 10) return cudaErrorInvalidValue;
+  const int per_point = fmt == kK1tF16 ? 2 : fmt == kK1tF16x2 ? 1 : 4;  // threads per point
   int g = (int)ceil_div(rows * per_point, 256);
   if (g > sm_count() * 8) g = sm_count() * 8;
   if (g < 1) g = 1;
-  if (fmt == kK1tF16)
+  if (fmt == kK1tF16x2)
+    k1t_pack16x2_kernel<<<g, 256, 0, s>>>(packed32, padded_dim(d), npts, rows, img);
+  else if (fmt == kK1tF16)
     k1t_pack16_kernel<<<g, 256, 0, s>>>(packed32, padded_dim(d), npts, rows, img);
   else
     k1t_pack_kernel<<<g, 256, 0, s>>>(packed32, padded_dim(d), npts, rows, img);

@@ -478,7 +478,7 @@ extern "C" int laker_pcg_solve(const laker_operator* op, const laker_precond* pc
   h.active = 1;
   cudaError_t e = cudaMemsetAsync(w.hdr, 0, kWsHeader, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(w.st, &h, sizeof(PcgState), cudaMemcpyHostToDevice, s);
-  const int tfmt = k1t_format(op->clamp);  // image format: the pack and every launch
+  const int tfmt = k1t_format(op->clamp, d);  // image format: the pack and every launch
   if (e == cudaSuccess && tc) e = launch_k1t_pack(op->packed32, n, d, w.img, sp.nb * sp.B, s, tfmt);
   if (e != cudaSuccess) return fail_cuda(e);
 

@@ -137,10 +137,13 @@ bool k1t_enabled(int d);
 // 8, three products each) or split FP16 (kind::f16, one K step of 16, three
 // products: H H' + Hs L' + L Hs' with H = fp16(v), L = fp16((v - H) 2^12),
 // Hs = fp16(H 2^-12)), used only for unclamped operators (every |e_k| < 9, so
-// no FP16 overflow).  k1t_format(clamp) is the format a pack and the launches
-// that read its image use (LAKER_VARIANT_K1T_LOGITS).
-constexpr int kK1tTf32 = 0, kK1tF16 = 1;
-int k1t_format(int clamp);
+// no FP16 overflow).  k1t_format(clamp, d) is the format a pack and the launches
+// that read its image use (LAKER_VARIANT_K1T_LOGITS).  For embeddings of at
+// most 10 (padded) dimensions the three split-FP16 products fit two K = 16
+// MMAs (kK1tF16x2): the correction products Hs L' and L Hs' fill H H''s
+// padding and a second K step, with the same FP16 values and products.
+constexpr int kK1tTf32 = 0, kK1tF16 = 1, kK1tF16x2 = 2;
+int k1t_format(int clamp, int d);
 size_t k1t_image_bytes(int64_t points);
 SymPlan k1t_plan(int64_t n);
 SymPlan k1t_plan_pairs(int64_t nb, int64_t npairs);
