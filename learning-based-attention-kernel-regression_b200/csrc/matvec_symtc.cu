@@ -30,6 +30,10 @@
 // H H' + Hs L' + L Hs' (= H H' + H lo' + lo H'), three kind::f16 MMAs of K =
 // 16 per row tile instead of six kind::tf32 MMAs of K = 8, half the operand
 // bytes (48 KB per side) and the f16 tensor rate.
+// Two-MMA FP16 format (the same, for at most 10 padded dimensions): four
+// variants, V0 = [H | Hs_0..], V1 = [Hs_P.. | L], W0 = [H' | L'_0..],
+// W1 = [L'_P.. | Hs'] (k1t_pack16x2_kernel), so that V0 W0 + V1 W1 gives the
+// same three products in two MMAs (32 KB per side).
 //
 // Roles in a CTA of 576 threads (one CTA per SM: 512 TMEM columns, up to
 // 221 KB of shared memory), no CTA-wide barrier in the main loop:
