@@ -7,7 +7,8 @@
 // 128-row tile and 64-point column slab
 //   S = E_r E_c^T      three kind::f16 MMAs of K = 16 from the split-FP16
 //                      operand image of the symmetric kernel (k1t_pack: rows
-//                      scaled by log2 e), M = 128, N = 64, into TMEM;
+//                      scaled by log2 e), two with its two-MMA format when
+//                      d <= 10, M = 128, N = 64, into TMEM;
 //   P = exp2(S)        CUDA cores: each thread loads 16 logits of its row from
 //                      TMEM, one MUFU ex2 each, splits P into TF32 hi + lo and
 //                      stores both back into TMEM (P never touches shared
@@ -72,7 +73,6 @@ constexpr uint32_t kFAccCol = 128u * kFBufs;
 // point (32-byte swizzle, K-major).
 constexpr uint32_t kFVar = 512u * 32u;
 constexpr uint32_t kFImgBlock = 128u * 1024u;
-constexpr uint32_t kFColSide = 3u * kFVar;
 constexpr uint32_t kFRowVar = kFRows * 32u;        // one variant of a row tile (4 KB)
 constexpr uint32_t kFColVar = kFSlab * 32u;        // one variant of a slab (2 KB)
 constexpr uint32_t kFRowOps = 3u * kFRowVar;       // 12 KB
@@ -102,7 +102,9 @@ __global__ void __launch_bounds__(kFThreads, 1)
     k2f_matvec(const uint8_t* __restrict__ rimg, int64_t m, const uint8_t* __restrict__ cimg,
                const uint8_t* __restrict__ ximg, int N, int S, K2fWork wk, float lam,
                const float* __restrict__ X, int64_t ldx, int k, float* __restrict__ Y,
-               int64_t ldy, float* __restrict__ part, int* status, const int* gate) {
+               int64_t ldy, float* __restrict__ part, int nv, int* status, const int* gate) {
+  // nv: operand variants per side of the image, 3 (split FP16) or 2 (the
+  // same products in two MMAs, d <= 10); the shared-memory slots hold three
   if (gate && *gate == 0) return;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* base =
@@ -178,9 +180,9 @@ __global__ void __launch_bounds__(kFThreads, 1)
         item_of(it, &rt, &ch, &sg, &s0, &s1);
         const int ab = (int)(ni & 1);
         if (!wait_or_abort(&a_empty[ab], (uint32_t)(((ni >> 1) & 1) ^ 1), status, abort)) break;
-        mbar_arrive_expect_tx(&a_full[ab], kFRowOps);
+        mbar_arrive_expect_tx(&a_full[ab], (uint32_t)nv * kFRowVar);
         const uint8_t* rsrc = rimg + (rt >> 2) * (int64_t)kFImgBlock + (rt & 3) * (int64_t)kFRowVar;
-        for (int v = 0; v < 3; ++v)
+        for (int v = 0; v < nv; ++v)
           bulk_g2s(sRow + ab * kFRowOps + v * kFRowVar, rsrc + v * kFVar, kFRowVar, &a_full[ab]);
         ++a_issued;
         bool ok = true;
@@ -191,12 +193,12 @@ __global__ void __launch_bounds__(kFThreads, 1)
             break;
           }
           uint8_t* dst = sStage + (size_t)st * sbytes;
-          mbar_arrive_expect_tx(&b_full[st], (uint32_t)(512 * N) + kFColOps);
+          mbar_arrive_expect_tx(&b_full[st], (uint32_t)(512 * N) + (uint32_t)nv * kFColVar);
           bulk_g2s(dst, ximg + ((int64_t)ch * 2 * wk.nslabs + 2 * s) * (int64_t)(256 * N),
                    (uint32_t)(512 * N), &b_full[st]);
           const uint8_t* csrc =
-              cimg + (s >> 3) * (int64_t)kFImgBlock + kFColSide + (s & 7) * (int64_t)kFColVar;
-          for (int v = 0; v < 3; ++v)
+              cimg + (s >> 3) * (int64_t)kFImgBlock + (int64_t)nv * kFVar + (s & 7) * (int64_t)kFColVar;
+          for (int v = 0; v < nv; ++v)
             bulk_g2s(dst + 512 * N + v * kFColVar, csrc + v * kFVar, kFColVar, &b_full[st]);
           ++b_issued;
         }
@@ -220,13 +222,19 @@ __global__ void __launch_bounds__(kFThreads, 1)
         const uint32_t ra = smem_u32(sRow + ab * kFRowOps);
         const uint32_t cb = smem_u32(sStage + (size_t)st * sbytes + 512 * N);
         const uint32_t d = tmem_base + (uint32_t)(buf * 128);
-        // H H' + Hs L' + L Hs' (variants 0 = H, 1 = L, 2 = Hs)
         mma_f16(d, kmajor_desc_raw(ra, kFSBO16, kFLayout16), kmajor_desc_raw(cb, kFSBO16, kFLayout16),
                 idesc_s, 0u);
-        mma_f16(d, kmajor_desc_raw(ra + 2 * kFRowVar, kFSBO16, kFLayout16),
-                kmajor_desc_raw(cb + kFColVar, kFSBO16, kFLayout16), idesc_s, 1u);
-        mma_f16(d, kmajor_desc_raw(ra + kFRowVar, kFSBO16, kFLayout16),
-                kmajor_desc_raw(cb + 2 * kFColVar, kFSBO16, kFLayout16), idesc_s, 1u);
+        if (nv == 2) {
+          // V0 W0 + V1 W1 = H H' + Hs L' + L Hs'
+          mma_f16(d, kmajor_desc_raw(ra + kFRowVar, kFSBO16, kFLayout16),
+                  kmajor_desc_raw(cb + kFColVar, kFSBO16, kFLayout16), idesc_s, 1u);
+        } else {
+          // H H' + Hs L' + L Hs' (variants 0 = H, 1 = L, 2 = Hs)
+          mma_f16(d, kmajor_desc_raw(ra + 2 * kFRowVar, kFSBO16, kFLayout16),
+                  kmajor_desc_raw(cb + kFColVar, kFSBO16, kFLayout16), idesc_s, 1u);
+          mma_f16(d, kmajor_desc_raw(ra + kFRowVar, kFSBO16, kFLayout16),
+                  kmajor_desc_raw(cb + 2 * kFColVar, kFSBO16, kFLayout16), idesc_s, 1u);
+        }
         mma_any = true;
         mma_commit(&s_full[buf]);
         return true;
@@ -449,8 +457,10 @@ cudaError_t launch_k2f(const float* rows32, int64_t m, const float* cols32, int6
   uint8_t* rimg = ws + L.rimg_off;
   uint8_t* cimg = ws + L.cimg_off;
   cudaError_t e = launch_pack_x32(X, n, ldx, k, N, 2 * wk.nslabs, ximg, gate, s);
-  if (e == cudaSuccess) e = launch_k1t_pack(rows32, m, d, rimg, round_up(m, 512), s, kK1tF16);
-  if (e == cudaSuccess && !same) e = launch_k1t_pack(cols32, n, d, cimg, round_up(n, 512), s, kK1tF16);
+  const int fmt = padded_dim(d) <= 10 ? kK1tF16x2 : kK1tF16;
+  const int nv = fmt == kK1tF16x2 ? 2 : 3;
+  if (e == cudaSuccess) e = launch_k1t_pack(rows32, m, d, rimg, round_up(m, 512), s, fmt);
+  if (e == cudaSuccess && !same) e = launch_k1t_pack(cols32, n, d, cimg, round_up(n, 512), s, fmt);
   if (e != cudaSuccess) return e;
   const int S = k2f_stages(N);
   const size_t smem = k2f_smem_bytes(N, S);
@@ -459,7 +469,7 @@ cudaError_t launch_k2f(const float* rows32, int64_t m, const float* cols32, int6
   if (e != cudaSuccess) return e;
   const int64_t grid = wk.items < (int64_t)sm_count() ? wk.items : (int64_t)sm_count();
   k2f_matvec<<<(unsigned)grid, kFThreads, smem, s>>>(rimg, m, cimg, ximg, N, S, wk, lam, X, ldx, k,
-                                                     Y, ldy, part, status, gate);
+                                                     Y, ldy, part, nv, status, gate);
   e = cudaGetLastError();
   if (e != cudaSuccess || wk.segs == 1) return e;
   return launch_seg_reduce(part, wk.segs, m, k, lam, X, ldx, Y, ldy, gate, s);
